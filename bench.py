@@ -1,0 +1,404 @@
+#!/usr/bin/env python
+"""Benchmark of the gSQG RK4 hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload forced1024|hires4096] [--precision float32|float64]
+
+Default workload ("forced1024"): forced-dissipative SQG (alpha = 1) at
+N = 1024: RingForcing(kf=40, dk=2, eps=0.1) with host-drawn phases
+(default_rng(1), one row per step), CombinedDamping(mu=0.1, kf=40, nu=1e-8,
+p=8), dt = 2e-4, initial field with random phases (seed 2) and spectrum
+~ k^4 exp(-(k/10)^2), rms 1.  The hyperviscous term is stiff for explicit
+RK4 (nu k_max^8 dt ~ 1e11), so the integrating-factor scheme is used.
+One "step" = one RK4 step of the field; metric = RK4 steps/s.
+
+"hires4096": gSQG alpha = 0.5 at N = 4096, ring kf=100, dk=2, eps=0.1,
+mu=0.05, nu=1e-20, p=8, dt=5e-5, k^-3 initial field (seed 3), plus two
+passive scalars (kappa = 1e-4) with mean-gradient forcing G = (1, 0).
+
+Timing: CUDA events on the launching stream; each timed step is bracketed by
+its own events and the L2 cache is flushed (a 256 MiB write) between steps
+outside the events.  Multi-GPU (torchrun): every rank runs an independent
+replica ("replicas only": a single field does not shard); the elapsed time is
+the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "forced1024": dict(N=1024, alpha=1.0, kf=40.0, dk=2.0, eps=0.1, mu=0.1, kf_damp=40.0, nu=1e-8, p=8, dt=2e-4,
+                       ic="k4exp", ic_seed=2, noise_seed=1, scalars=0),
+    "hires4096": dict(N=4096, alpha=0.5, kf=100.0, dk=2.0, eps=0.1, mu=0.05, kf_damp=100.0, nu=1e-20, p=8, dt=5e-5,
+                      ic="kminus3", ic_seed=3, noise_seed=4, scalars=2),
+}
+
+
+def initial_field(O, g, w):
+    if w["ic"] == "k4exp":
+        return O.random_phase_field(g, lambda k: k**4 * np.exp(-((k / 10.0) ** 2)), w["ic_seed"])
+    return O.random_phase_field(g, lambda k: k ** (-3.0), w["ic_seed"])
+
+
+def bytes_per_launch(N, w_bytes):
+    """Algorithmic bytes of each pass per launch (model stated in DESIGN.md).
+
+    P = N^2, half array = (N/2+1) N complex = ~w P bytes, full spectrum = 2 w P.
+    column pass: reads 4 half arrays, writes 1 half array.
+    row stage pass (IF-RK4, ring modes only in the stage buffer):
+      s=1: jh + theta_n + acc(w) + 4 half out     = 1 + 2 + 2 + 4   half units
+      s=2,3: jh + theta_n + acc(r) + acc(w) + 4   = 1 + 2 + 2 + 2 + 4
+      s=4: jh + acc(r) + theta_out(w) + 4         = 1 + 2 + 2 + 4
+    row inverse pass (start of a step): theta (2) + 4 half out.
+    """
+    half = (N // 2 + 1) * N * 2 * w_bytes
+    return {
+        "col_theta": 5 * half,
+        "row_stage": (9 + 11 + 11 + 9) / 4 * half,
+        "row_inverse": 6 * half,
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(workload, prec, kernel):
+    p = os.path.join(ROOT, "profiles", "traffic_per_launch.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return d.get(f"{workload}/{prec}/{kernel}")
+
+
+def cpu_baseline(w, seconds=12.0, warm=1):
+    """The float64 CPU restatement of the reference algorithm (9 complex
+    FFTs per RHS, forcing rescale with 2 more), IF-RK4, scipy.fft threads =
+    all host cores; a bounded number of steps."""
+    from oracle import sqg_oracle as O
+
+    cores = len(os.sched_getaffinity(0))
+    O.set_fft_workers(cores)
+    g = O.make_grid(w["N"], 2 * np.pi)
+    s = O.gSQGSolver(g, w["alpha"], 0.0, w["p"], scheme="ifrk4")
+    ring = O.RingForcing(w["kf"], w["dk"], w["eps"])
+    damp = O.CombinedDamping(w["mu"], w["kf_damp"], w["nu"], w["p"])
+    st = s.initialize(theta0=initial_field(O, g, w))
+    rng = np.random.default_rng(w["noise_seed"])
+    n_ring = O.ring_mode_count(g, w["kf"], w["dk"])
+    for _ in range(warm):
+        st = O.step_forced(s, st, w["dt"], ring, rng.uniform(0, 2 * np.pi, n_ring), damp)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        st = O.step_forced(s, st, w["dt"], ring, rng.uniform(0, 2 * np.pi, n_ring), damp)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or n >= 200:
+            break
+    O.set_fft_workers(1)
+    return {"value": n / el, "unit": "steps/s", "cores": cores, "kind": "port",
+            "sample": f"{n} IF-RK4 steps of the {w['N']}^2 workload (float64 oracle, scipy.fft workers={cores})"}
+
+
+def run_reference(args, w):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import sqg_oracle as O
+
+    cores = len(os.sched_getaffinity(0))
+    O.set_fft_workers(cores)
+    g = O.make_grid(w["N"], 2 * np.pi)
+    s = O.gSQGSolver(g, w["alpha"], 0.0, w["p"], scheme="ifrk4")
+    ring = O.RingForcing(w["kf"], w["dk"], w["eps"])
+    damp = O.CombinedDamping(w["mu"], w["kf_damp"], w["nu"], w["p"])
+    st = s.initialize(theta0=initial_field(O, g, w))
+    rng = np.random.default_rng(w["noise_seed"])
+    n_ring = O.ring_mode_count(g, w["kf"], w["dk"])
+    step = lambda st: O.step_forced(s, st, w["dt"], ring, rng.uniform(0, 2 * np.pi, n_ring), damp)  # noqa: E731
+    t0 = time.perf_counter()
+    for _ in range(max(args.warmup, 1)):
+        st = step(st)
+    t_step = (time.perf_counter() - t0) / max(args.warmup, 1)
+    k = max(2, min(args.steps, int(120.0 / max(t_step, 1e-6))))
+    t0 = time.perf_counter()
+    for _ in range(k):
+        st = step(st)
+    el = time.perf_counter() - t0
+    v = k / el
+    line = {
+        "impl": "reference", "metric": "RK4 steps/s", "value": v, "unit": "steps/s", "n_gpus": args.gpus,
+        "steps": k, "warmup": max(args.warmup, 1), "ms_per_step": 1e3 * el / k, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "N": w["N"], "scheme": "ifrk4", "parallelism": "replicas"},
+        "cpu_baseline": {"value": v, "unit": "steps/s", "cores": cores, "kind": "port",
+                         "sample": f"{k} IF-RK4 steps, float64 oracle restatement of the reference algorithm, "
+                                   f"scipy.fft workers={cores}"},
+        "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="forced1024", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="float32", choices=["float32", "float64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variants", default="auto", help="extra measured variants: auto|none")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, w)
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from oracle import sqg_oracle as O  # initial field generator (host, seeded)
+    import pygsquig_b200 as P
+    from pygsquig_b200.build import build
+
+    if rank == 0:
+        build()
+    if world > 1:
+        dist.barrier()
+
+    def measure(workload, prec, steps, warmup, with_e2e, with_clocks):
+        w = WORKLOADS[workload]
+        N = w["N"]
+        g = P.make_grid(N, 2 * np.pi)
+        ring = P.RingForcing(w["kf"], w["dk"], w["eps"])
+        damp = P.CombinedDamping(w["mu"], w["kf_damp"], w["nu"], w["p"])
+        if w["scalars"]:
+            s = P.gSQGSolverWithScalars(g, w["alpha"], 0.0, w["p"], precision=prec, scheme="ifrk4",
+                                        passive_scalars={f"c{i}": {"kappa": 1e-4, "source": P.MeanGradientSource(1.0, 0.0)}
+                                                         for i in range(w["scalars"])})
+        else:
+            s = P.gSQGSolver(g, w["alpha"], 0.0, w["p"], precision=prec, scheme="ifrk4")
+        go = O.make_grid(N, 2 * np.pi)
+        th0 = initial_field(O, go, w)
+        sinit = None
+        if w["scalars"]:
+            x, y = go.x, go.y
+            sinit = {f"c{i}": np.exp(-((x - 2.0 - i) ** 2 + (y - 3.0) ** 2) / (2 * 0.3**2)) for i in range(w["scalars"])}
+            st = s.initialize(theta0=th0, scalar_init=sinit)
+        else:
+            st = s.initialize(theta0=th0)
+        n_ring = ring.n_modes(g)
+        rng = np.random.default_rng(w["noise_seed"] + 1000 * rank)
+        total = warmup + steps
+        noise_host = torch.from_numpy(rng.uniform(0, 2 * np.pi, size=(total, n_ring))).pin_memory()
+        noise_dev = noise_host.to("cuda")
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        stream = torch.cuda.current_stream()
+        dt = w["dt"]
+
+        def one(i, st):
+            return s.step(st, dt, forcing=ring.bind(noise_dev[i], dt, g), damping=damp)
+
+        for i in range(warmup):
+            st = one(i, st)
+        torch.cuda.synchronize()
+        pl = s.plan(damp, ring)
+        # ---- device-resident timed region ----
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local) if with_clocks else None
+        if sampler:
+            sampler.__enter__()
+        launches = 0
+        for k in range(steps):
+            evs[k][0].record(stream)
+            st = one(warmup + k, st)
+            evs[k][1].record(stream)
+            launches += pl.last_launch_count()
+            if w["scalars"]:
+                pass
+            flush.zero_()
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.__exit__()
+        ms = sum(a.elapsed_time(b) for a, b in evs)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+        th = st["theta_hat"]
+        finite = bool(torch.isfinite(torch.view_as_real(th)).all().item())
+        res = {"ms": ms, "steps": steps, "launches": launches, "finite": finite,
+               "clocks": sampler.summary() if sampler else None}
+        # ---- per-kernel breakdown (events around each launch) ----
+        pl.set_timing(True)
+        nk = min(steps, 10)
+        for k in range(nk):
+            st = one(warmup + k, st)
+            flush.zero_()
+        torch.cuda.synchronize()
+        res["kernels"] = pl.timing_read()
+        pl.set_timing(False)
+        res["kernel_steps"] = nk
+        # ---- end to end through the public API with host buffers ----
+        if with_e2e:
+            out_host = torch.empty(1, dtype=torch.float64).pin_memory()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for k in range(steps):
+                ph = noise_host[warmup + k].to("cuda", non_blocking=True)  # H2D of this step's input
+                st = s.step(st, dt, forcing=ring.bind(ph, dt, g), damping=damp)
+                half_theta2 = 0.5 * pl.inner(st["theta_hat"], st["theta_hat"])  # D2H of the step's metric
+                out_host[0] = half_theta2
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ems = e0.elapsed_time(e1)
+            if world > 1:
+                t = torch.tensor([ems], device="cuda", dtype=torch.float64)
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                ems = float(t.item())
+            res["e2e"] = {"value": world * steps / (ems / 1e3), "unit": "steps/s",
+                          "h2d_bytes_per_step": int(n_ring * 8), "d2h_bytes_per_step": 8}
+        del flush
+        return res
+
+    peak, peak_kind = measured_peaks()
+    prec = args.precision
+    main_res = measure(args.workload, prec, args.steps, args.warmup, True, True)
+    wb = 4 if prec == "float32" else 8
+    N = w["N"]
+    bpl = bytes_per_launch(N, wb)
+    kern = {}
+    for name, (ms, cnt) in main_res["kernels"].items():
+        if cnt == 0:
+            continue
+        avg = ms / cnt
+        e = {"launches": cnt, "avg_us": 1e3 * avg, "share": None}
+        if name in bpl:
+            e["algorithmic_bytes"] = bpl[name]
+            e["achieved_gbs"] = bpl[name] / (avg / 1e3) / 1e9
+        kern[name] = e
+    tot = sum(v["avg_us"] * v["launches"] for v in kern.values())
+    for v in kern.values():
+        v["share"] = v["avg_us"] * v["launches"] / tot
+    dom = max((k for k in kern if "achieved_gbs" in kern[k]), key=lambda k: kern[k]["share"])
+    value = world * main_res["steps"] / (main_res["ms"] / 1e3)
+    ms_per_step = main_res["ms"] / main_res["steps"]
+    model_bytes = 88 * wb * N * N  # SURVEY model: 88 w N^2 per RK4 step
+    line = {
+        "metric": "RK4 steps/s", "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if prec == "float32" else "f64",
+        "data": "synthetic (seeded initial field and host-drawn ring phases)",
+        "config": {"workload": args.workload, "N": N, "alpha": w["alpha"], "scheme": "ifrk4",
+                   "ring": [w["kf"], w["dk"], w["eps"]], "damping": [w["mu"], w["kf_damp"], w["nu"], w["p"]],
+                   "dt": w["dt"], "passive_scalars": w["scalars"], "parallelism": f"replicas x{world}",
+                   "l2": "flushed between timed steps (256 MiB write outside the step events)"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["achieved_gbs"], "peak": peak,
+                     "unit": "GB/s", "frac": kern[dom]["achieved_gbs"] / peak, "peak_kind": peak_kind,
+                     "traffic": ncu_traffic(args.workload, prec, dom)},
+        "step_model": {"model_bytes_per_step": model_bytes, "model_gbs": model_bytes / (ms_per_step / 1e3) / 1e9,
+                       "frac_of_peak": model_bytes / (ms_per_step / 1e3) / 1e9 / peak},
+        "kernels": kern,
+        "gpu_launches": main_res["launches"],
+        "clocks": main_res["clocks"],
+        "e2e": main_res["e2e"],
+        "finite": main_res["finite"],
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(w)
+    if args.variants == "auto":
+        other = "float64" if prec == "float32" else "float32"
+        v = measure(args.workload, other, max(10, args.steps // 2), 3, False, False)
+        line["variant_" + other] = {"value": world * v["steps"] / (v["ms"] / 1e3), "unit": "steps/s",
+                                    "ms_per_step": v["ms"] / v["steps"], "finite": v["finite"],
+                                    "kernels": {k: {"launches": c, "avg_us": 1e3 * m / max(c, 1)}
+                                                for k, (m, c) in v["kernels"].items() if c}}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

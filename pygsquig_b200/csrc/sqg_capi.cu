@@ -1,0 +1,984 @@
+// sqg_capi.cu -- plan management, host-side tables and the extern "C" entry
+// points declared in include/sqg.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/sqg.h"
+#include "sqg_aux.cuh"
+
+using namespace sqg;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define SQG_CUDA(call)                                                              \
+  do {                                                                              \
+    cudaError_t err__ = (call);                                                     \
+    if (err__ != cudaSuccess)                                                       \
+      return fail(SQG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(err__)); \
+  } while (0)
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+struct sqg_plan {
+  sqg_desc d;
+  int N, H, log2N;
+  size_t csize;  // bytes per complex element
+  int akind;
+  // host tables
+  std::vector<double> k1d;
+  std::vector<RowTab> rows;
+  std::vector<int> ring_pos, ring_mirror;
+  int herm_ord[4];
+  std::vector<double> edges;
+  int n_bins;
+  double ou_decay, ou_vf;
+  // workspace
+  unsigned char* ws = nullptr;
+  size_t ws_bytes = 0;
+  size_t off_k1d, off_k1t, off_tw, off_rows, off_ring_pos, off_ring_mirror, off_ringF, off_ring_scale,
+      off_ou_state, off_ou_init, off_status, off_step_ctr, off_acc, off_stage, off_xh, off_jh, off_uv, off_xs, off_js,
+      off_sacc, off_sstage, off_src, off_part, off_edges, off_phys, off_total;
+  int n_src_buf;
+  bool ready = false;
+  bool stage_begun = false;
+  int64_t launches = 0;
+  // CUDA graph of one steady-state step (multistep)
+  cudaGraphExec_t graph_exec = nullptr;
+  const void* graph_theta = nullptr;
+  const double* graph_phases = nullptr;
+  double graph_dt = 0.0;
+  cudaStream_t graph_stream = nullptr;
+  // per-launch CUDA-event timing (bench instrumentation)
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_pool;
+  struct Rec { int kind; cudaEvent_t a, b; };
+  std::vector<Rec> recs;
+  size_t ev_used = 0;
+};
+
+namespace {
+
+constexpr int kPartBlocks = 296;  // 2 x 148 SMs
+
+template <typename P> P* wsp(const sqg_plan* pl, size_t off) { return reinterpret_cast<P*>(pl->ws + off); }
+
+// fftfreq(N, d=L/N) * 2 * pi, evaluated in the order numpy uses so that the
+// values are bit-identical to the reference's grid (grid.py:88-95).
+std::vector<double> wavenumbers(int N, double L) {
+  const double dx = L / N;
+  const double val = 1.0 / (N * dx);
+  std::vector<double> k(N);
+  const int npos = (N - 1) / 2 + 1;
+  for (int i = 0; i < N; ++i) {
+    const long m = i < npos ? i : (long)i - N;
+    k[i] = (((double)m * val) * 2.0) * M_PI;
+  }
+  return k;
+}
+
+int alpha_kind(double a) {
+  if (a == 0.0) return AK_ZERO;
+  if (a == 1.0) return AK_ONE;
+  if (a == 0.5) return AK_HALF;
+  if (a == 1.5) return AK_THREEHALF;
+  if (a == 2.0) return AK_TWO;
+  if (a == -1.0) return AK_MINUSONE;
+  return AK_GENERAL;
+}
+
+void build_tables(sqg_plan* pl) {
+  const int N = pl->N, H = pl->H;
+  const sqg_desc& d = pl->d;
+  pl->k1d = wavenumbers(N, d.L);
+  const std::vector<double>& k = pl->k1d;
+  // dealias cutoff (2/3) * pi * N / L, grid.py:102-105
+  const double k_max = M_PI * N / d.L;
+  const double cutoff = (2.0 / 3.0) * k_max;
+  const double drag_half = d.kf_damp / 2;
+  const double ring_half = d.ring_dk / 2;
+  pl->rows.assign(N, RowTab{});
+  pl->ring_pos.clear();
+  for (int ix = 0; ix < N; ++ix) {
+    RowTab& rt = pl->rows[ix];
+    const double kx2 = k[ix] * k[ix];
+    rt.dmax = -1;
+    rt.dragmax = -1;
+    int lo = H + 1, hi = -1;
+    for (int my = 0; my <= H; ++my) {
+      const double ky = k[my == H ? H : my];
+      const double km = std::sqrt(kx2 + ky * ky);
+      if (km < cutoff) rt.dmax = my;
+      if (d.has_damping && d.mu != 0.0 && km < drag_half) rt.dragmax = my;
+      if (d.has_ring && std::fabs(km - d.ring_kf) <= ring_half) {
+        if (my < lo) lo = my;
+        if (my > hi) hi = my;
+      }
+    }
+    rt.pos_lo = 1; rt.pos_hi = 0; rt.neg_lo = 1; rt.neg_hi = 0;  // empty
+    rt.row_start = (int)pl->ring_pos.size();
+    if (hi >= lo) {
+      const int plo = lo, phi = std::min(hi, H - 1);
+      if (phi >= plo) { rt.pos_lo = plo; rt.pos_hi = phi; }
+      const int nlo = std::max(N - hi, H), nhi = N - std::max(lo, 1);
+      if (nhi >= nlo) { rt.neg_lo = nlo; rt.neg_hi = nhi; }
+      for (int iy = rt.pos_lo; iy <= rt.pos_hi; ++iy) pl->ring_pos.push_back(ix * N + iy);
+      for (int iy = rt.neg_lo; iy <= rt.neg_hi; ++iy) pl->ring_pos.push_back(ix * N + iy);
+    }
+  }
+  const int n = (int)pl->ring_pos.size();
+  pl->ring_mirror.assign(n, 0);
+  for (int i = 0; i < n; ++i) {
+    const int ix = pl->ring_pos[i] / N, iy = pl->ring_pos[i] % N;
+    const int mx = (N - ix) % N, my = (N - iy) % N;
+    const RowTab& rt = pl->rows[mx];
+    int o = -1;
+    if (my >= rt.pos_lo && my <= rt.pos_hi) o = rt.row_start + (my - rt.pos_lo);
+    else if (my >= rt.neg_lo && my <= rt.neg_hi)
+      o = rt.row_start + (rt.pos_hi >= rt.pos_lo ? rt.pos_hi - rt.pos_lo + 1 : 0) + (my - rt.neg_lo);
+    pl->ring_mirror[i] = o;
+  }
+  const int hpos[4] = {0, H * N, H, H * N + H};
+  for (int h = 0; h < 4; ++h) {
+    pl->herm_ord[h] = -1;
+    for (int i = 0; i < n; ++i)
+      if (pl->ring_pos[i] == hpos[h]) pl->herm_ord[h] = i;
+  }
+  // spectrum bins: numpy linspace(0, k_max, n_bins + 1)
+  const double dk = 2 * M_PI / d.L;
+  const double kmx = N * dk / 2;
+  pl->n_bins = std::min(N / 4, 64);
+  pl->edges.assign(pl->n_bins + 1, 0.0);
+  const double step = kmx / pl->n_bins;
+  for (int i = 0; i <= pl->n_bins; ++i) pl->edges[i] = i * step + 0.0;
+  pl->edges[pl->n_bins] = kmx;
+  // OU coefficients (ring_forcing.py:112-113)
+  if (d.has_ring && d.ring_tau_f > 0) {
+    pl->ou_decay = std::exp(-0.0 / d.ring_tau_f);  // set per dt at step time
+    pl->ou_vf = 0.0;
+  }
+}
+
+void layout(sqg_plan* pl) {
+  const size_t N = pl->N, H = pl->H, cs = pl->csize;
+  const size_t n = std::max<size_t>(pl->ring_pos.size(), 1);
+  const size_t full = N * N * cs;
+  const size_t half = (H + 1) * N * cs;
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t r = o; o += align256(bytes); return r; };
+  pl->off_k1d = take(N * sizeof(double));
+  pl->off_k1t = take(N * cs / 2);
+  pl->off_tw = take(N * cs);
+  pl->off_rows = take(N * sizeof(RowTab));
+  pl->off_ring_pos = take(n * sizeof(int));
+  pl->off_ring_mirror = take(n * sizeof(int));
+  pl->off_ringF = take(4 * n * sizeof(double2));
+  pl->off_ring_scale = take(4 * sizeof(double));
+  pl->off_ou_state = take(n * sizeof(double2));
+  pl->off_ou_init = take(sizeof(int));
+  pl->off_status = take(sizeof(unsigned));
+  pl->off_step_ctr = take(sizeof(int));
+  pl->off_edges = take(65 * sizeof(double));
+  pl->off_part = take((size_t)kPartBlocks * 64 * sizeof(double) + 64 * sizeof(double));
+  pl->off_acc = take(full);
+  pl->off_stage = take(full);
+  pl->off_xh = take(4 * half);
+  pl->off_jh = take(half);
+  pl->off_phys = take(N * N * (cs / 2));
+  const int ns = pl->d.n_scalars;
+  pl->n_src_buf = 0;
+  for (int s = 0; s < ns; ++s) pl->n_src_buf += pl->d.mean_gradient[s] ? 1 : 0;
+  pl->off_uv = take(ns ? full : 0);
+  pl->off_xs = take(ns ? 2 * half : 0);
+  pl->off_js = take(ns ? half : 0);
+  pl->off_sacc = take(ns ? full : 0);
+  pl->off_sstage = take(ns ? full : 0);
+  pl->off_src = take((size_t)pl->n_src_buf * half);
+  pl->off_total = o;
+}
+
+KP make_kp(const sqg_plan* pl, double dt) {
+  KP kp;
+  std::memset(&kp, 0, sizeof(kp));
+  const sqg_desc& d = pl->d;
+  kp.N = pl->N;
+  kp.H = pl->H;
+  kp.k1d = wsp<double>(pl, pl->off_k1d);
+  kp.k1t = pl->ws + pl->off_k1t;
+  kp.tw = pl->ws + pl->off_tw;
+  kp.rows = wsp<RowTab>(pl, pl->off_rows);
+  kp.inv_n2 = 1.0 / ((double)pl->N * (double)pl->N);
+  kp.alpha = d.alpha;
+  kp.akind = pl->akind;
+  kp.scheme = d.scheme;
+  kp.nu_s = d.nu_p;
+  kp.ps = d.p;
+  kp.nu_d = d.has_damping ? d.nu_damp : 0.0;
+  kp.pd = d.has_damping ? d.p_damp : 8;
+  kp.mu = d.has_damping ? d.mu : 0.0;
+  kp.dt = dt;
+  kp.n_ring = (int)pl->ring_pos.size();
+  kp.ring_on = (d.has_ring && kp.n_ring > 0) ? 1 : 0;
+  kp.ringF = wsp<double2>(pl, pl->off_ringF);
+  kp.status = wsp<unsigned>(pl, pl->off_status);
+  return kp;
+}
+
+// ---- compile-time launch shapes ----
+constexpr int rows_per_cta(int log2n) { return (1 << log2n) / 8 >= 128 ? 1 : 128 / ((1 << log2n) / 8); }
+constexpr int pairs_per_cta(int log2n) {
+  return ((1 << log2n) / 8 >= 256) ? 1
+         : (256 / ((1 << log2n) / 8) > 16 ? ((1 << log2n) / 2 < 16 ? (1 << log2n) / 2 : 16)
+                                          : 256 / ((1 << log2n) / 8));
+}
+
+template <typename T, int L>
+size_t row_smem() { return (size_t)rows_per_cta(L) * 2 * (1 << L) * sizeof(typename Cplx<T>::type); }
+template <typename T, int L>
+size_t col_smem() { return (size_t)pairs_per_cta(L) * 2 * (1 << L) * sizeof(typename Cplx<T>::type); }
+
+template <typename T, int L>
+cudaError_t launch_row_t(const KP& kp, const RowArgs& a, cudaStream_t st) {
+  constexpr int N = 1 << L, RPC = rows_per_cta(L), G = N / 8;
+  const int grid = (N / 2 + 1 + RPC - 1) / RPC;
+  k_row<T, L, RPC><<<grid, RPC * G, row_smem<T, L>(), st>>>(kp, a);
+  return cudaGetLastError();
+}
+template <typename T, int L>
+cudaError_t launch_col_t(const KP& kp, const ColArgs& a, cudaStream_t st, bool ring_only) {
+  constexpr int N = 1 << L, NP = pairs_per_cta(L), G = N / 8;
+  int grid = ring_only ? 1 : N / (2 * NP) + (a.ring_cta ? 1 : 0);
+  k_col<T, L, NP><<<grid, NP * G, col_smem<T, L>(), st>>>(kp, a);
+  return cudaGetLastError();
+}
+template <typename T, int L>
+cudaError_t set_attrs_t() {
+  constexpr int RPC = rows_per_cta(L), NP = pairs_per_cta(L);
+  cudaError_t e = cudaFuncSetAttribute(k_row<T, L, RPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)row_smem<T, L>());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_col<T, L, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem<T, L>());
+}
+
+#define SQG_DISPATCH(LOG2N, FN, ...)                  \
+  switch (LOG2N) {                                    \
+    case 3: return FN<T, 3>(__VA_ARGS__);             \
+    case 4: return FN<T, 4>(__VA_ARGS__);             \
+    case 5: return FN<T, 5>(__VA_ARGS__);             \
+    case 6: return FN<T, 6>(__VA_ARGS__);             \
+    case 7: return FN<T, 7>(__VA_ARGS__);             \
+    case 8: return FN<T, 8>(__VA_ARGS__);             \
+    case 9: return FN<T, 9>(__VA_ARGS__);             \
+    case 10: return FN<T, 10>(__VA_ARGS__);           \
+    case 11: return FN<T, 11>(__VA_ARGS__);           \
+    case 12: return FN<T, 12>(__VA_ARGS__);           \
+    default: return cudaErrorInvalidValue;            \
+  }
+
+template <typename T>
+cudaError_t launch_row_p(int log2n, const KP& kp, const RowArgs& a, cudaStream_t st) {
+  SQG_DISPATCH(log2n, launch_row_t, kp, a, st);
+}
+template <typename T>
+cudaError_t launch_col_p(int log2n, const KP& kp, const ColArgs& a, cudaStream_t st, bool ring_only) {
+  SQG_DISPATCH(log2n, launch_col_t, kp, a, st, ring_only);
+}
+template <typename T>
+cudaError_t set_attrs_p(int log2n) {
+  SQG_DISPATCH(log2n, set_attrs_t);
+}
+
+// Timing kinds reported by sqg_timing_read.
+enum { TK_ROW_P1 = 0, TK_ROW_STAGE = 1, TK_COL_THETA = 2, TK_ROW_SCALAR = 3, TK_COL_SCALAR = 4, TK_OTHER = 5,
+       TK_COUNT = 6 };
+
+cudaEvent_t next_event(sqg_plan* pl) {
+  if (pl->ev_used == pl->ev_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    pl->ev_pool.push_back(e);
+  }
+  return pl->ev_pool[pl->ev_used++];
+}
+
+template <typename F>
+cudaError_t timed(sqg_plan* pl, int kind, cudaStream_t st, F&& f) {
+  pl->launches++;
+  if (!pl->timing) return f();
+  cudaEvent_t a = next_event(pl), b = next_event(pl);
+  cudaEventRecord(a, st);
+  cudaError_t e = f();
+  cudaEventRecord(b, st);
+  pl->recs.push_back({kind, a, b});
+  return e;
+}
+
+cudaError_t launch_row(sqg_plan* pl, const KP& kp, const RowArgs& a, cudaStream_t st) {
+  const int kind = a.fmode == FM_SCAL ? TK_ROW_SCALAR : (a.rmode == RM_P1 ? TK_ROW_P1 : (a.rmode == RM_STAGE ? TK_ROW_STAGE : TK_OTHER));
+  return timed(pl, kind, st, [&] {
+    return pl->d.precision == SQG_F64 ? launch_row_p<double>(pl->log2N, kp, a, st)
+                                      : launch_row_p<float>(pl->log2N, kp, a, st);
+  });
+}
+cudaError_t launch_col(sqg_plan* pl, const KP& kp, const ColArgs& a, cudaStream_t st, bool ring_only = false) {
+  const int kind = a.cmode == CM_THETA ? TK_COL_THETA : (a.cmode == CM_SCAL ? TK_COL_SCALAR : TK_OTHER);
+  return timed(pl, kind, st, [&] {
+    return pl->d.precision == SQG_F64 ? launch_col_p<double>(pl->log2N, kp, a, st, ring_only)
+                                      : launch_col_p<float>(pl->log2N, kp, a, st, ring_only);
+  });
+}
+
+RowArgs base_row(sqg_plan* pl) {
+  RowArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.xh = pl->ws + pl->off_xh;
+  a.jh = pl->ws + pl->off_jh;
+  a.acc = pl->ws + pl->off_acc;
+  a.st_in = pl->ws + pl->off_stage;
+  a.st_out = pl->ws + pl->off_stage;
+  a.fmode = FM_THETA;
+  return a;
+}
+
+ColArgs base_col(sqg_plan* pl) {
+  ColArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.cmode = CM_THETA;
+  a.xh = pl->ws + pl->off_xh;
+  a.jh = pl->ws + pl->off_jh;
+  return a;
+}
+
+// fills the ring-forcing part of the column args for stage s
+void ring_args(sqg_plan* pl, ColArgs& a, int s, const void* theta_s, const double* phases, double dt,
+               const int* step_ctr) {
+  const sqg_desc& d = pl->d;
+  a.ring_cta = 1;
+  a.stage = s;
+  a.ring_theta = theta_s;
+  a.phases = phases;
+  a.ring_pos = wsp<int>(pl, pl->off_ring_pos);
+  a.ring_mirror = wsp<int>(pl, pl->off_ring_mirror);
+  a.ringF = wsp<double2>(pl, pl->off_ringF);
+  a.ou_state = wsp<double2>(pl, pl->off_ou_state);
+  a.ou_init = wsp<int>(pl, pl->off_ou_init);
+  a.ring_amp = d.ring_amplitude;
+  a.ring_eps = d.ring_epsilon;
+  a.ring_ou = d.ring_tau_f > 0 ? 1 : 0;
+  if (a.ring_ou) {
+    a.ou_decay = std::exp(-dt / d.ring_tau_f);
+    a.ou_vf = std::sqrt(1 - a.ou_decay * a.ou_decay);
+  }
+  for (int h = 0; h < 4; ++h) a.herm_ord[h] = pl->herm_ord[h];
+  a.ring_scale_out = wsp<double>(pl, pl->off_ring_scale);
+  (void)step_ctr;
+}
+
+bool ring_active(const sqg_plan* pl) { return pl->d.has_ring && !pl->ring_pos.empty(); }
+
+int check_ready(const sqg_plan* pl) {
+  if (!pl) return fail(SQG_ERR_INVALID, "null plan");
+  if (!pl->ready) return fail(SQG_ERR_WORKSPACE, "workspace not set (call sqg_plan_set_workspace)");
+  return SQG_OK;
+}
+
+// One RK4 stage: column pass (with ring reduction) then row pass.
+int run_stage(sqg_plan* pl, int s, const void* th_n, void* th_out, double dt, const void* extra,
+              const double* phases, int stage_write, int do_p1, cudaStream_t st) {
+  KP kp = make_kp(pl, dt);
+  ColArgs ca = base_col(pl);
+  if (ring_active(pl)) {
+    if (!phases) return fail(SQG_ERR_INVALID, "ring forcing needs phases");
+    ring_args(pl, ca, s, s == 1 ? th_n : (const void*)(pl->ws + pl->off_stage), phases, dt, nullptr);
+  }
+  SQG_CUDA(launch_col(pl, kp, ca, st));
+  RowArgs ra = base_row(pl);
+  ra.rmode = RM_STAGE;
+  ra.stage = s;
+  ra.th_n = th_n;
+  ra.th_out = th_out;
+  ra.extra = extra;
+  ra.stage_write = stage_write;
+  ra.do_p1 = do_p1;
+  SQG_CUDA(launch_row(pl, kp, ra, st));
+  return SQG_OK;
+}
+
+int stage_write_mode(const sqg_plan* pl, bool generic) {
+  if (generic) return SW_FULL;
+  const bool lin = (pl->d.nu_p != 0.0) || (pl->d.has_damping && (pl->d.mu != 0.0 || pl->d.nu_damp != 0.0));
+  if (pl->d.scheme == SQG_EXPLICIT_RK4 && lin) return SW_FULL;
+  if (ring_active(pl)) return SW_RING;
+  return SW_NONE;
+}
+
+int run_p1(sqg_plan* pl, const void* th, int fmode, void* xh, cudaStream_t st, double dt = 0.0) {
+  KP kp = make_kp(pl, dt);
+  RowArgs ra = base_row(pl);
+  ra.rmode = RM_P1;
+  ra.fmode = fmode;
+  ra.th_n = th;
+  ra.do_p1 = 1;
+  if (xh) ra.xh = xh;
+  SQG_CUDA(launch_row(pl, kp, ra, st));
+  return SQG_OK;
+}
+
+int one_step(sqg_plan* pl, const void* th_in, void* th_out, double dt, const double* phases, bool p1_first,
+             cudaStream_t st) {
+  int rc;
+  if (p1_first) {
+    if ((rc = run_p1(pl, th_in, FM_THETA, nullptr, st)) != SQG_OK) return rc;
+  }
+  const int sw = stage_write_mode(pl, false);
+  // stages 1-3 read th_in as theta_n; stage 4 writes th_out (may alias th_in)
+  for (int s = 1; s <= 4; ++s) {
+    if ((rc = run_stage(pl, s, th_in, th_out, dt, nullptr, phases, sw, s < 4 ? 1 : 0, st)) != SQG_OK) return rc;
+  }
+  return SQG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sqg_version(void) { return 1; }
+
+const char* sqg_last_error_string(void) { return g_last_error.c_str(); }
+
+int sqg_plan_create(const sqg_desc* desc, sqg_plan** out) {
+  if (!desc || !out) return fail(SQG_ERR_INVALID, "null argument");
+  const sqg_desc& d = *desc;
+  int log2n = 0;
+  while ((1 << log2n) < d.N) ++log2n;
+  if (d.N % 2 != 0) return fail(SQG_ERR_INVALID, "N must be even, got " + std::to_string(d.N));
+  if ((1 << log2n) != d.N || d.N < 8 || d.N > 4096)
+    return fail(SQG_ERR_INVALID, "N must be a power of two in [8, 4096], got " + std::to_string(d.N));
+  if (!(d.alpha >= -2 && d.alpha <= 2)) return fail(SQG_ERR_INVALID, "alpha must be in [-2, 2], got " + std::to_string(d.alpha));
+  if (d.p != 2 && d.p != 4 && d.p != 8) return fail(SQG_ERR_INVALID, "p must be 2, 4, or 8, got " + std::to_string(d.p));
+  if (d.has_damping && d.p_damp != 2 && d.p_damp != 4 && d.p_damp != 8)
+    return fail(SQG_ERR_INVALID, "p must be 2, 4, or 8, got " + std::to_string(d.p_damp));
+  if (d.precision != SQG_F64 && d.precision != SQG_F32) return fail(SQG_ERR_INVALID, "bad precision");
+  if (d.scheme != SQG_EXPLICIT_RK4 && d.scheme != SQG_IF_RK4) return fail(SQG_ERR_INVALID, "bad scheme");
+  if (!(d.L > 0)) return fail(SQG_ERR_INVALID, "L must be positive");
+  if (d.n_scalars < 0 || d.n_scalars > SQG_MAX_SCALARS) return fail(SQG_ERR_INVALID, "n_scalars out of range");
+  sqg_plan* pl = new sqg_plan();
+  pl->d = d;
+  pl->N = d.N;
+  pl->H = d.N / 2;
+  pl->log2N = log2n;
+  pl->csize = d.precision == SQG_F64 ? 16 : 8;
+  pl->akind = alpha_kind(d.alpha);
+  build_tables(pl);
+  layout(pl);
+  *out = pl;
+  return SQG_OK;
+}
+
+int sqg_plan_destroy(sqg_plan* pl) {
+  if (!pl) return SQG_OK;
+  if (pl->graph_exec) cudaGraphExecDestroy(pl->graph_exec);
+  for (cudaEvent_t e : pl->ev_pool) cudaEventDestroy(e);
+  delete pl;
+  return SQG_OK;
+}
+
+int sqg_plan_workspace_bytes(const sqg_plan* pl, size_t* bytes) {
+  if (!pl || !bytes) return fail(SQG_ERR_INVALID, "null argument");
+  *bytes = pl->off_total;
+  return SQG_OK;
+}
+
+int sqg_plan_buffer(const sqg_plan* pl, int32_t which, size_t* offset, size_t* bytes) {
+  if (!pl || !offset || !bytes) return fail(SQG_ERR_INVALID, "null argument");
+  const size_t full = (size_t)pl->N * pl->N * pl->csize;
+  switch (which) {
+    case SQG_BUF_STAGE: *offset = pl->off_stage; *bytes = full; break;
+    case SQG_BUF_UV: *offset = pl->off_uv; *bytes = pl->d.n_scalars ? full : 0; break;
+    case SQG_BUF_RING_FORCE: *offset = pl->off_ringF; *bytes = pl->ring_pos.size() * sizeof(double2); break;
+    case SQG_BUF_STATUS: *offset = pl->off_status; *bytes = sizeof(unsigned); break;
+    default: return fail(SQG_ERR_INVALID, "unknown buffer");
+  }
+  return SQG_OK;
+}
+
+int sqg_plan_set_workspace(sqg_plan* pl, void* ws, size_t bytes, void* stream) {
+  if (!pl) return fail(SQG_ERR_INVALID, "null plan");
+  if (!ws) return fail(SQG_ERR_WORKSPACE, "null workspace");
+  if (bytes < pl->off_total) return fail(SQG_ERR_WORKSPACE, "workspace too small");
+  if (((uintptr_t)ws) & 255) return fail(SQG_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+  cudaStream_t st = (cudaStream_t)stream;
+  pl->ws = (unsigned char*)ws;
+  pl->ws_bytes = bytes;
+  const int N = pl->N;
+  // host staging of the tables
+  std::vector<unsigned char> host(pl->off_acc, 0);
+  std::memcpy(host.data() + pl->off_k1d, pl->k1d.data(), N * sizeof(double));
+  if (pl->d.precision == SQG_F64) {
+    std::memcpy(host.data() + pl->off_k1t, pl->k1d.data(), N * sizeof(double));
+    std::vector<double2> tw(N);
+    for (int k = 0; k < N; ++k) {
+      const long double ang = 2.0L * 3.14159265358979323846264338327950288L * k / N;
+      tw[k] = make_double2((double)cosl(ang), (double)-sinl(ang));
+    }
+    std::memcpy(host.data() + pl->off_tw, tw.data(), N * sizeof(double2));
+  } else {
+    std::vector<float> kf(N);
+    for (int i = 0; i < N; ++i) kf[i] = (float)pl->k1d[i];
+    std::memcpy(host.data() + pl->off_k1t, kf.data(), N * sizeof(float));
+    std::vector<float2> tw(N);
+    for (int k = 0; k < N; ++k) {
+      const long double ang = 2.0L * 3.14159265358979323846264338327950288L * k / N;
+      tw[k] = make_float2((float)cosl(ang), (float)-sinl(ang));
+    }
+    std::memcpy(host.data() + pl->off_tw, tw.data(), N * sizeof(float2));
+  }
+  std::memcpy(host.data() + pl->off_rows, pl->rows.data(), N * sizeof(RowTab));
+  if (!pl->ring_pos.empty()) {
+    std::memcpy(host.data() + pl->off_ring_pos, pl->ring_pos.data(), pl->ring_pos.size() * sizeof(int));
+    std::memcpy(host.data() + pl->off_ring_mirror, pl->ring_mirror.data(), pl->ring_mirror.size() * sizeof(int));
+  }
+  std::memcpy(host.data() + pl->off_edges, pl->edges.data(), pl->edges.size() * sizeof(double));
+  SQG_CUDA(cudaMemcpyAsync(ws, host.data(), pl->off_acc, cudaMemcpyHostToDevice, st));
+  SQG_CUDA(cudaStreamSynchronize(st));
+  if (pl->d.precision == SQG_F64) { SQG_CUDA(set_attrs_p<double>(pl->log2N)); }
+  else { SQG_CUDA(set_attrs_p<float>(pl->log2N)); }
+  if (pl->graph_exec) {
+    cudaGraphExecDestroy(pl->graph_exec);
+    pl->graph_exec = nullptr;
+  }
+  pl->ready = true;
+  return SQG_OK;
+}
+
+int sqg_ring_mode_count(const sqg_plan* pl, int32_t* n) {
+  if (!pl || !n) return fail(SQG_ERR_INVALID, "null argument");
+  *n = pl->d.has_ring ? (int32_t)pl->ring_pos.size() : 0;
+  return SQG_OK;
+}
+
+int sqg_ring_modes(const sqg_plan* pl, int32_t* ix, int32_t* iy) {
+  if (!pl || !ix || !iy) return fail(SQG_ERR_INVALID, "null argument");
+  for (size_t i = 0; i < pl->ring_pos.size(); ++i) {
+    ix[i] = pl->ring_pos[i] / pl->N;
+    iy[i] = pl->ring_pos[i] % pl->N;
+  }
+  return SQG_OK;
+}
+
+// Host copies of the grid tables (CPU-side checks of the masks).
+int sqg_plan_host_tables(const sqg_plan* pl, double* k1d, int32_t* dmax, int32_t* dragmax) {
+  if (!pl) return fail(SQG_ERR_INVALID, "null plan");
+  for (int i = 0; i < pl->N; ++i) {
+    if (k1d) k1d[i] = pl->k1d[i];
+    if (dmax) dmax[i] = pl->rows[i].dmax;
+    if (dragmax) dragmax[i] = pl->rows[i].dragmax;
+  }
+  return SQG_OK;
+}
+
+int sqg_rhs(sqg_plan* pl, const void* theta, void* rhs, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!theta || !rhs) return fail(SQG_ERR_INVALID, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  pl->launches = 0;
+  if ((rc = run_p1(pl, theta, FM_THETA, nullptr, st)) != SQG_OK) return rc;
+  KP kp = make_kp(pl, 0.0);
+  kp.ring_on = 0;
+  ColArgs ca = base_col(pl);
+  SQG_CUDA(launch_col(pl, kp, ca, st));
+  RowArgs ra = base_row(pl);
+  ra.rmode = RM_RHS;
+  ra.stage = 1;
+  ra.th_n = theta;
+  ra.rhs_out = rhs;
+  ra.do_p1 = 0;
+  SQG_CUDA(launch_row(pl, kp, ra, st));
+  return SQG_OK;
+}
+
+int sqg_step(sqg_plan* pl, const void* th_in, void* th_out, double dt, const double* phases, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!th_in || !th_out) return fail(SQG_ERR_INVALID, "null pointer");
+  pl->launches = 0;
+  return one_step(pl, th_in, th_out, dt, phases, true, (cudaStream_t)stream);
+}
+
+int sqg_stage_begin(sqg_plan* pl, const void* th_in, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  pl->launches = 0;
+  rc = run_p1(pl, th_in, FM_THETA, nullptr, (cudaStream_t)stream);
+  if (rc == SQG_OK) pl->stage_begun = true;
+  return rc;
+}
+
+int sqg_stage(sqg_plan* pl, int32_t s, const void* th_in, void* th_out, double dt, const void* extra,
+              const double* phases, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!pl->stage_begun) return fail(SQG_ERR_STATE, "sqg_stage before sqg_stage_begin");
+  if (s < 1 || s > 4) return fail(SQG_ERR_INVALID, "stage must be 1..4");
+  rc = run_stage(pl, s, th_in, th_out, dt, extra, phases, stage_write_mode(pl, true), s < 4 ? 1 : 0,
+                 (cudaStream_t)stream);
+  if (s == 4) pl->stage_begun = false;
+  return rc;
+}
+
+int sqg_multistep(sqg_plan* pl, void* theta, int32_t n_steps, double dt, const double* phases, int32_t use_graph,
+                  void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!theta) return fail(SQG_ERR_INVALID, "null pointer");
+  if (n_steps < 0) return fail(SQG_ERR_INVALID, "n_steps must be >= 0");
+  if (n_steps == 0) return SQG_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n_ring = (int)pl->ring_pos.size();
+  const bool ring = ring_active(pl);
+  if (ring && !phases) return fail(SQG_ERR_INVALID, "ring forcing needs phases");
+  pl->launches = 0;
+  if ((rc = run_p1(pl, theta, FM_THETA, nullptr, st)) != SQG_OK) return rc;
+  const int sw = stage_write_mode(pl, false);
+  if (!use_graph || ring || pl->timing) {
+    // ring phases change every step; plain launches
+    for (int n = 0; n < n_steps; ++n) {
+      const double* ph = ring ? phases + (size_t)n * n_ring : nullptr;
+      for (int s = 1; s <= 4; ++s) {
+        const int do_p1 = (s < 4 || n + 1 < n_steps) ? 1 : 0;
+        if ((rc = run_stage(pl, s, theta, theta, dt, nullptr, ph, sw, do_p1, st)) != SQG_OK) return rc;
+      }
+    }
+    return SQG_OK;
+  }
+  // CUDA graph of one steady-state step (stage 4 also prepares the next step)
+  if (!pl->graph_exec || pl->graph_theta != theta || pl->graph_dt != dt || pl->graph_stream != st) {
+    if (pl->graph_exec) {
+      cudaGraphExecDestroy(pl->graph_exec);
+      pl->graph_exec = nullptr;
+    }
+    cudaGraph_t g;
+    SQG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int64_t saved = pl->launches;
+    for (int s = 1; s <= 4 && rc == SQG_OK; ++s) rc = run_stage(pl, s, theta, theta, dt, nullptr, nullptr, sw, 1, st);
+    cudaError_t ce = cudaStreamEndCapture(st, &g);
+    pl->launches = saved;
+    if (rc != SQG_OK) return rc;
+    if (ce != cudaSuccess) return fail(SQG_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&pl->graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) return fail(SQG_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(ce));
+    pl->graph_theta = theta;
+    pl->graph_dt = dt;
+    pl->graph_stream = st;
+  }
+  for (int n = 0; n < n_steps; ++n) {
+    SQG_CUDA(cudaGraphLaunch(pl->graph_exec, st));
+    pl->launches += 8;
+  }
+  return SQG_OK;
+}
+
+int sqg_velocity(sqg_plan* pl, const void* theta, void* u, void* v, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!theta || !u || !v) return fail(SQG_ERR_INVALID, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((rc = run_p1(pl, theta, FM_VEL, nullptr, st)) != SQG_OK) return rc;
+  KP kp = make_kp(pl, 0.0);
+  ColArgs ca = base_col(pl);
+  ca.cmode = CM_VEL;
+  ca.out0 = u;
+  ca.out1 = v;
+  SQG_CUDA(launch_col(pl, kp, ca, st));
+  return SQG_OK;
+}
+
+int sqg_to_physical(sqg_plan* pl, const void* field_hat, void* field, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!field_hat || !field) return fail(SQG_ERR_INVALID, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((rc = run_p1(pl, field_hat, FM_PHYS1, nullptr, st)) != SQG_OK) return rc;
+  KP kp = make_kp(pl, 0.0);
+  ColArgs ca = base_col(pl);
+  ca.cmode = CM_PHYS1;
+  ca.out0 = field;
+  SQG_CUDA(launch_col(pl, kp, ca, st));
+  return SQG_OK;
+}
+
+static int linear_term(sqg_plan* pl, const void* theta, void* out, double nu, int pw, double mu, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!theta || !out) return fail(SQG_ERR_INVALID, "null pointer");
+  KP kp = make_kp(pl, 0.0);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (pl->d.precision == SQG_F64)
+    k_linear<double><<<4 * kPartBlocks, 256, 0, st>>>(kp, nu, pw, mu, (const double2*)theta, (double2*)out);
+  else
+    k_linear<float><<<4 * kPartBlocks, 256, 0, st>>>(kp, nu, pw, mu, (const float2*)theta, (float2*)out);
+  SQG_CUDA(cudaGetLastError());
+  return SQG_OK;
+}
+
+int sqg_damping(sqg_plan* pl, const void* theta, void* out, void* stream) {
+  if (pl && !pl->d.has_damping) return fail(SQG_ERR_INVALID, "plan carries no damping");
+  return linear_term(pl, theta, out, pl ? pl->d.nu_damp : 0.0, pl ? pl->d.p_damp : 8, pl ? pl->d.mu : 0.0, stream);
+}
+
+int sqg_hyperviscosity(sqg_plan* pl, const void* theta, void* out, void* stream) {
+  return linear_term(pl, theta, out, pl ? pl->d.nu_p : 0.0, pl ? pl->d.p : 8, 0.0, stream);
+}
+
+int sqg_to_spectral(sqg_plan* pl, const void* field, void* field_hat, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!field || !field_hat) return fail(SQG_ERR_INVALID, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  KP kp = make_kp(pl, 0.0);
+  ColArgs ca = base_col(pl);
+  ca.cmode = CM_FWD;
+  ca.in_real = field;
+  SQG_CUDA(launch_col(pl, kp, ca, st));
+  RowArgs ra = base_row(pl);
+  ra.rmode = RM_SPEC;
+  ra.rhs_out = field_hat;
+  SQG_CUDA(launch_row(pl, kp, ra, st));
+  return SQG_OK;
+}
+
+int sqg_inner(sqg_plan* pl, const void* a, const void* b, double* out, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!a || !b || !out) return fail(SQG_ERR_INVALID, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  double* part = wsp<double>(pl, pl->off_part);
+  if (pl->d.precision == SQG_F64)
+    k_inner_partial<double><<<kPartBlocks, 256, 0, st>>>(pl->N, (const double2*)a, (const double2*)b, part);
+  else
+    k_inner_partial<float><<<kPartBlocks, 256, 0, st>>>(pl->N, (const float2*)a, (const float2*)b, part);
+  k_var_final<<<1, 256, 0, st>>>(kPartBlocks, pl->N, part, out);
+  SQG_CUDA(cudaGetLastError());
+  return SQG_OK;
+}
+
+int sqg_ring_forcing(sqg_plan* pl, const void* theta, const double* phases, double dt, void* out, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!theta || !out) return fail(SQG_ERR_INVALID, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t full = (size_t)pl->N * pl->N * pl->csize;
+  SQG_CUDA(cudaMemsetAsync(out, 0, full, st));
+  if (!ring_active(pl)) return SQG_OK;
+  if (!phases) return fail(SQG_ERR_INVALID, "ring forcing needs phases");
+  KP kp = make_kp(pl, dt);
+  ColArgs ca = base_col(pl);
+  ring_args(pl, ca, 1, theta, phases, dt, nullptr);
+  SQG_CUDA(launch_col(pl, kp, ca, st, true));
+  const int n = (int)pl->ring_pos.size();
+  if (pl->d.precision == SQG_F64)
+    k_ring_scatter<double><<<(n + 255) / 256, 256, 0, st>>>(n, wsp<int>(pl, pl->off_ring_pos), kp.ringF, (double2*)out);
+  else
+    k_ring_scatter<float><<<(n + 255) / 256, 256, 0, st>>>(n, wsp<int>(pl, pl->off_ring_pos), kp.ringF, (float2*)out);
+  SQG_CUDA(cudaGetLastError());
+  return SQG_OK;
+}
+
+int sqg_diagnostics(sqg_plan* pl, const void* theta, double* out, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!theta || !out) return fail(SQG_ERR_INVALID, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  KP kp = make_kp(pl, 0.0);
+  double* part = wsp<double>(pl, pl->off_part);
+  double* maxv = part + (size_t)kPartBlocks * 64;
+  // max |theta| in physical space
+  void* phys = pl->ws + pl->off_phys;
+  if ((rc = sqg_to_physical(pl, theta, phys, stream)) != SQG_OK) return rc;
+  const size_t nn = (size_t)pl->N * pl->N;
+  if (pl->d.precision == SQG_F64)
+    k_absmax_partial<double><<<kPartBlocks, 256, 0, st>>>((const double*)phys, nn, part);
+  else
+    k_absmax_partial<float><<<kPartBlocks, 256, 0, st>>>((const float*)phys, nn, part);
+  k_absmax_final<<<1, 256, 0, st>>>(kPartBlocks, part, maxv);
+  if (pl->d.precision == SQG_F64)
+    k_diag_partial<double><<<kPartBlocks, 256, 0, st>>>(kp, (const double2*)theta, part);
+  else
+    k_diag_partial<float><<<kPartBlocks, 256, 0, st>>>(kp, (const float2*)theta, part);
+  k_diag_final<<<1, 256, 0, st>>>(kPartBlocks, pl->N, part, maxv, out);
+  SQG_CUDA(cudaGetLastError());
+  return SQG_OK;
+}
+
+int sqg_energy_spectrum(sqg_plan* pl, const void* theta, double* out, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!theta || !out) return fail(SQG_ERR_INVALID, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  KP kp = make_kp(pl, 0.0);
+  double* part = wsp<double>(pl, pl->off_part);
+  const double* edges = wsp<double>(pl, pl->off_edges);
+  if (pl->d.precision == SQG_F64)
+    k_spectrum_partial<double><<<kPartBlocks, 256, 0, st>>>(kp, (const double2*)theta, edges, pl->n_bins, part);
+  else
+    k_spectrum_partial<float><<<kPartBlocks, 256, 0, st>>>(kp, (const float2*)theta, edges, pl->n_bins, part);
+  k_spectrum_final<<<1, 64, 0, st>>>(kPartBlocks, pl->n_bins, part, edges, out);
+  SQG_CUDA(cudaGetLastError());
+  return SQG_OK;
+}
+
+int sqg_scalar_variance(sqg_plan* pl, const void* s_hat, double* out, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!s_hat || !out) return fail(SQG_ERR_INVALID, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  double* part = wsp<double>(pl, pl->off_part);
+  if (pl->d.precision == SQG_F64)
+    k_var_partial<double><<<kPartBlocks, 256, 0, st>>>(pl->N, (const double2*)s_hat, part);
+  else
+    k_var_partial<float><<<kPartBlocks, 256, 0, st>>>(pl->N, (const float2*)s_hat, part);
+  k_var_final<<<1, 256, 0, st>>>(kPartBlocks, pl->N, part, out);
+  SQG_CUDA(cudaGetLastError());
+  return SQG_OK;
+}
+
+int sqg_scalars_step(sqg_plan* pl, const void* theta_new, const void* const* s_in, void* const* s_out, double dt,
+                     void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  const int ns = pl->d.n_scalars;
+  if (ns == 0) return SQG_OK;
+  if (!theta_new || !s_in || !s_out) return fail(SQG_ERR_INVALID, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  KP kp = make_kp(pl, dt);
+  kp.ring_on = 0;
+  void* uv = pl->ws + pl->off_uv;
+  void* xs = pl->ws + pl->off_xs;
+  void* js = pl->ws + pl->off_js;
+  // 1. velocity of theta_new (frozen over the scalar stages) and the
+  //    mean-gradient source spectra
+  {
+    RowArgs ra = base_row(pl);
+    ra.rmode = RM_P1;
+    ra.fmode = FM_VEL;
+    ra.th_n = theta_new;
+    ra.do_p1 = 1;
+    int k = 0;
+    for (int s = 0; s < ns; ++s) {
+      if (!pl->d.mean_gradient[s]) continue;
+      ra.src_out[k] = pl->ws + pl->off_src + (size_t)k * (pl->H + 1) * pl->N * pl->csize;
+      ra.gx[k] = pl->d.grad_x[s];
+      ra.gy[k] = pl->d.grad_y[s];
+      ++k;
+    }
+    ra.n_src = k;
+    SQG_CUDA(launch_row(pl, kp, ra, st));
+    ColArgs ca = base_col(pl);
+    ca.cmode = CM_VEL;
+    ca.out0 = uv;
+    ca.out1 = nullptr;
+    SQG_CUDA(launch_col(pl, kp, ca, st));
+  }
+  // 2. RK4 of each scalar
+  int ksrc = 0;
+  for (int s = 0; s < ns; ++s) {
+    const void* src = nullptr;
+    if (pl->d.mean_gradient[s]) {
+      src = pl->ws + pl->off_src + (size_t)ksrc * (pl->H + 1) * pl->N * pl->csize;
+      ++ksrc;
+    }
+    RowArgs p1 = base_row(pl);
+    p1.rmode = RM_P1;
+    p1.fmode = FM_SCAL;
+    p1.th_n = s_in[s];
+    p1.do_p1 = 1;
+    p1.xh = xs;
+    SQG_CUDA(launch_row(pl, kp, p1, st));
+    const bool explicit_lin = pl->d.scheme == SQG_EXPLICIT_RK4 && pl->d.kappa[s] != 0.0;
+    for (int stg = 1; stg <= 4; ++stg) {
+      ColArgs ca = base_col(pl);
+      ca.cmode = CM_SCAL;
+      ca.xh = xs;
+      ca.jh = js;
+      ca.uv = uv;
+      SQG_CUDA(launch_col(pl, kp, ca, st));
+      RowArgs ra = base_row(pl);
+      ra.rmode = RM_STAGE;
+      ra.fmode = FM_SCAL;
+      ra.stage = stg;
+      ra.th_n = s_in[s];
+      ra.th_out = s_out[s];
+      ra.acc = pl->ws + pl->off_sacc;
+      ra.st_in = pl->ws + pl->off_sstage;
+      ra.st_out = pl->ws + pl->off_sstage;
+      ra.jh = js;
+      ra.xh = xs;
+      ra.kappa = pl->d.kappa[s];
+      ra.src_h = src;
+      ra.stage_write = explicit_lin ? SW_FULL : SW_NONE;
+      ra.do_p1 = stg < 4 ? 1 : 0;
+      KP kps = kp;
+      kps.ring_on = 0;
+      SQG_CUDA(launch_row(pl, kps, ra, st));
+    }
+  }
+  return SQG_OK;
+}
+
+int sqg_check_status(sqg_plan* pl, uint32_t* flags, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!flags) return fail(SQG_ERR_INVALID, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned h = 0;
+  SQG_CUDA(cudaMemcpyAsync(&h, pl->ws + pl->off_status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  SQG_CUDA(cudaStreamSynchronize(st));
+  SQG_CUDA(cudaMemsetAsync(pl->ws + pl->off_status, 0, sizeof(unsigned), st));
+  *flags = h;
+  return SQG_OK;
+}
+
+int sqg_set_timing(sqg_plan* pl, int32_t enable) {
+  if (!pl) return fail(SQG_ERR_INVALID, "null plan");
+  pl->timing = enable != 0;
+  pl->recs.clear();
+  pl->ev_used = 0;
+  return SQG_OK;
+}
+
+int sqg_timing_read(sqg_plan* pl, double* ms, int64_t* count, int32_t nkinds) {
+  if (!pl || !ms || !count) return fail(SQG_ERR_INVALID, "null argument");
+  for (int k = 0; k < nkinds; ++k) { ms[k] = 0.0; count[k] = 0; }
+  for (const auto& r : pl->recs) {
+    SQG_CUDA(cudaEventSynchronize(r.b));
+    float t = 0.f;
+    SQG_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+    if (r.kind < nkinds) { ms[r.kind] += t; count[r.kind] += 1; }
+  }
+  pl->recs.clear();
+  pl->ev_used = 0;
+  return SQG_OK;
+}
+
+int sqg_last_launch_count(const sqg_plan* pl, int64_t* n) {
+  if (!pl || !n) return fail(SQG_ERR_INVALID, "null argument");
+  *n = pl->launches;
+  return SQG_OK;
+}
+
+}  // extern "C"
