@@ -72,50 +72,71 @@ def bytes_per_launch(N, w_bytes):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle sampling while the timed region runs."""
+    """nvidia-smi clocks/throttle sampling around the timed region.
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    Started before the warm-up steps (a reader thread timestamps every
+    sample); the caller keeps the same load running for about a second after
+    the timed steps so that the samples bracket the timed region.
+    """
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index):
         self.idx = gpu_index
         self.p = None
+        self.rows = []
 
-    def __enter__(self):
+    def start(self):
+        import threading
+
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.p = None
+            return self
+
+        def reader():
+            for line in self.p.stdout:
+                self.rows.append((time.time(), line.strip()))
+
+        self.t = threading.Thread(target=reader, daemon=True)
+        self.t.start()
+        t0 = time.time()
+        while not self.rows and time.time() - t0 < 5.0:
+            time.sleep(0.05)
         return self
 
-    def __exit__(self, *a):
-        self.out = ""
+    def stop(self):
         if self.p is not None:
             self.p.terminate()
             try:
-                self.out, _ = self.p.communicate(timeout=5)
+                self.p.wait(timeout=5)
             except Exception:
                 self.p.kill()
 
-    def summary(self):
-        rows = []
-        for line in (self.out or "").strip().splitlines():
+    def summary(self, t_from, t_to):
+        vals = []
+        for t, line in self.rows:
+            if not (t_from <= t <= t_to):
+                continue
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 7:
                 continue
             try:
-                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+                vals.append((float(parts[0]), float(parts[1]), float(parts[2]), parts[3:7]))
             except ValueError:
                 continue
-        if not rows:
+        if not vals:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
-        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
-                "reasons": reasons, "samples": len(rows)}
+        reasons = sorted({names[i] for *_, r in vals for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(v[0] for v in vals), "sm_max_mhz": max(v[1] for v in vals),
+                "power_w_max": max(v[2] for v in vals), "reasons": reasons, "samples": len(vals),
+                "window": "timed steps plus 1 s of the same load after them"}
 
 
 def measured_peaks():
@@ -273,6 +294,7 @@ def main():
         def one(i, st):
             return s.step(st, dt, forcing=ring.bind(noise_dev[i], dt, g), damping=damp)
 
+        sampler = ClockSampler(local).start() if with_clocks else None
         for i in range(warmup):
             st = one(i, st)
         torch.cuda.synchronize()
@@ -282,9 +304,7 @@ def main():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
-        sampler = ClockSampler(local) if with_clocks else None
-        if sampler:
-            sampler.__enter__()
+        t_wall0 = time.time()
         launches = 0
         for k in range(steps):
             evs[k][0].record(stream)
@@ -295,8 +315,15 @@ def main():
                 pass
             flush.zero_()
         torch.cuda.synchronize()
+        t_wall1 = time.time()
         if sampler:
-            sampler.__exit__()
+            # same load for ~1 s more, so the clock samples bracket the timed steps
+            stx = st
+            while time.time() - t_wall1 < 1.0:
+                for k in range(min(steps, 20)):
+                    stx = one(warmup + k, stx)
+                torch.cuda.synchronize()
+            sampler.stop()
         ms = sum(a.elapsed_time(b) for a, b in evs)
         if world > 1:
             t = torch.tensor([ms], device="cuda", dtype=torch.float64)
@@ -306,7 +333,7 @@ def main():
         th = st["theta_hat"]
         finite = bool(torch.isfinite(torch.view_as_real(th)).all().item())
         res = {"ms": ms, "steps": steps, "launches": launches, "finite": finite,
-               "clocks": sampler.summary() if sampler else None}
+               "clocks": sampler.summary(t_wall0 - 0.1, time.time()) if sampler else None}
         # ---- per-kernel breakdown (events around each launch) ----
         pl.set_timing(True)
         nk = min(steps, 10)

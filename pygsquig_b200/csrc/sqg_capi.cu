@@ -51,7 +51,7 @@ struct sqg_plan {
   size_t ws_bytes = 0;
   size_t off_k1d, off_k1t, off_tw, off_rows, off_ring_pos, off_ring_mirror, off_ringF, off_ring_scale,
       off_ou_state, off_ou_init, off_status, off_step_ctr, off_acc, off_stage, off_xh, off_jh, off_uv, off_xs, off_js,
-      off_sacc, off_sstage, off_src, off_part, off_edges, off_phys, off_total;
+      off_sacc, off_sstage, off_src, off_part, off_edges, off_phys, off_state, off_ctl, off_total;
   int n_src_buf;
   bool ready = false;
   bool stage_begun = false;
@@ -61,7 +61,8 @@ struct sqg_plan {
   const void* graph_theta = nullptr;
   const double* graph_phases = nullptr;
   double graph_dt = 0.0;
-  cudaStream_t graph_stream = nullptr;
+  cudaStream_t cap_stream = nullptr;  // plan-owned stream the graph is captured on and replayed on
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   // per-launch CUDA-event timing (bench instrumentation)
   bool timing = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -198,6 +199,8 @@ void layout(sqg_plan* pl) {
   pl->off_xh = take(4 * half);
   pl->off_jh = take(half);
   pl->off_phys = take(N * N * (cs / 2));
+  pl->off_state = take(full);
+  pl->off_ctl = take(sizeof(RingCtl));
   const int ns = pl->d.n_scalars;
   pl->n_src_buf = 0;
   for (int s = 0; s < ns; ++s) pl->n_src_buf += pl->d.mean_gradient[s] ? 1 : 0;
@@ -364,7 +367,7 @@ ColArgs base_col(sqg_plan* pl) {
 
 // fills the ring-forcing part of the column args for stage s
 void ring_args(sqg_plan* pl, ColArgs& a, int s, const void* theta_s, const double* phases, double dt,
-               const int* step_ctr) {
+               RingCtl* ctl) {
   const sqg_desc& d = pl->d;
   a.ring_cta = 1;
   a.stage = s;
@@ -384,7 +387,7 @@ void ring_args(sqg_plan* pl, ColArgs& a, int s, const void* theta_s, const doubl
   }
   for (int h = 0; h < 4; ++h) a.herm_ord[h] = pl->herm_ord[h];
   a.ring_scale_out = wsp<double>(pl, pl->off_ring_scale);
-  (void)step_ctr;
+  a.ctl = ctl;
 }
 
 bool ring_active(const sqg_plan* pl) { return pl->d.has_ring && !pl->ring_pos.empty(); }
@@ -397,12 +400,12 @@ int check_ready(const sqg_plan* pl) {
 
 // One RK4 stage: column pass (with ring reduction) then row pass.
 int run_stage(sqg_plan* pl, int s, const void* th_n, void* th_out, double dt, const void* extra,
-              const double* phases, int stage_write, int do_p1, cudaStream_t st) {
+              const double* phases, int stage_write, int do_p1, cudaStream_t st, RingCtl* ctl = nullptr) {
   KP kp = make_kp(pl, dt);
   ColArgs ca = base_col(pl);
   if (ring_active(pl)) {
-    if (!phases) return fail(SQG_ERR_INVALID, "ring forcing needs phases");
-    ring_args(pl, ca, s, s == 1 ? th_n : (const void*)(pl->ws + pl->off_stage), phases, dt, nullptr);
+    if (!phases && !ctl) return fail(SQG_ERR_INVALID, "ring forcing needs phases");
+    ring_args(pl, ca, s, s == 1 ? th_n : (const void*)(pl->ws + pl->off_stage), phases, dt, ctl);
   }
   SQG_CUDA(launch_col(pl, kp, ca, st));
   RowArgs ra = base_row(pl);
@@ -492,6 +495,9 @@ int sqg_plan_destroy(sqg_plan* pl) {
   if (!pl) return SQG_OK;
   if (pl->graph_exec) cudaGraphExecDestroy(pl->graph_exec);
   for (cudaEvent_t e : pl->ev_pool) cudaEventDestroy(e);
+  if (pl->cap_stream) cudaStreamDestroy(pl->cap_stream);
+  if (pl->ev_in) cudaEventDestroy(pl->ev_in);
+  if (pl->ev_out) cudaEventDestroy(pl->ev_out);
   delete pl;
   return SQG_OK;
 }
@@ -560,7 +566,7 @@ int sqg_plan_set_workspace(sqg_plan* pl, void* ws, size_t bytes, void* stream) {
     cudaGraphExecDestroy(pl->graph_exec);
     pl->graph_exec = nullptr;
   }
-  pl->ready = true;
+  pl->ready = true;  // (graph captures reference workspace addresses)
   return SQG_OK;
 }
 
@@ -652,10 +658,9 @@ int sqg_multistep(sqg_plan* pl, void* theta, int32_t n_steps, double dt, const d
   const bool ring = ring_active(pl);
   if (ring && !phases) return fail(SQG_ERR_INVALID, "ring forcing needs phases");
   pl->launches = 0;
-  if ((rc = run_p1(pl, theta, FM_THETA, nullptr, st)) != SQG_OK) return rc;
   const int sw = stage_write_mode(pl, false);
-  if (!use_graph || ring || pl->timing) {
-    // ring phases change every step; plain launches
+  if (!use_graph || pl->timing) {
+    if ((rc = run_p1(pl, theta, FM_THETA, nullptr, st)) != SQG_OK) return rc;
     for (int n = 0; n < n_steps; ++n) {
       const double* ph = ring ? phases + (size_t)n * n_ring : nullptr;
       for (int s = 1; s <= 4; ++s) {
@@ -665,31 +670,52 @@ int sqg_multistep(sqg_plan* pl, void* theta, int32_t n_steps, double dt, const d
     }
     return SQG_OK;
   }
-  // CUDA graph of one steady-state step (stage 4 also prepares the next step)
-  if (!pl->graph_exec || pl->graph_theta != theta || pl->graph_dt != dt || pl->graph_stream != st) {
+  // CUDA graph of one steady-state step, captured on the plan's own stream
+  // over the plan's state buffer (stage 4 also prepares the next step; the
+  // ring phases of step n are read through the device control block).
+  void* state = pl->ws + pl->off_state;
+  RingCtl* ctl = wsp<RingCtl>(pl, pl->off_ctl);
+  const size_t full = (size_t)pl->N * pl->N * pl->csize;
+  if (!pl->cap_stream) {
+    SQG_CUDA(cudaStreamCreateWithFlags(&pl->cap_stream, cudaStreamNonBlocking));
+    SQG_CUDA(cudaEventCreateWithFlags(&pl->ev_in, cudaEventDisableTiming));
+    SQG_CUDA(cudaEventCreateWithFlags(&pl->ev_out, cudaEventDisableTiming));
+  }
+  cudaStream_t cs = pl->cap_stream;
+  if (!pl->graph_exec || pl->graph_dt != dt) {
     if (pl->graph_exec) {
       cudaGraphExecDestroy(pl->graph_exec);
       pl->graph_exec = nullptr;
     }
     cudaGraph_t g;
-    SQG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    SQG_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     int64_t saved = pl->launches;
-    for (int s = 1; s <= 4 && rc == SQG_OK; ++s) rc = run_stage(pl, s, theta, theta, dt, nullptr, nullptr, sw, 1, st);
-    cudaError_t ce = cudaStreamEndCapture(st, &g);
+    for (int s = 1; s <= 4 && rc == SQG_OK; ++s)
+      rc = run_stage(pl, s, state, state, dt, nullptr, nullptr, sw, 1, cs, ring ? ctl : nullptr);
+    cudaError_t ce = cudaStreamEndCapture(cs, &g);
     pl->launches = saved;
     if (rc != SQG_OK) return rc;
     if (ce != cudaSuccess) return fail(SQG_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
     ce = cudaGraphInstantiate(&pl->graph_exec, g, 0);
     cudaGraphDestroy(g);
     if (ce != cudaSuccess) return fail(SQG_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(ce));
-    pl->graph_theta = theta;
     pl->graph_dt = dt;
-    pl->graph_stream = st;
   }
+  SQG_CUDA(cudaMemcpyAsync(state, theta, full, cudaMemcpyDeviceToDevice, st));
+  if (ring) {
+    k_set_ctl<<<1, 1, 0, st>>>(ctl, phases);
+    SQG_CUDA(cudaGetLastError());
+  }
+  if ((rc = run_p1(pl, state, FM_THETA, nullptr, st)) != SQG_OK) return rc;
+  SQG_CUDA(cudaEventRecord(pl->ev_in, st));
+  SQG_CUDA(cudaStreamWaitEvent(cs, pl->ev_in, 0));
   for (int n = 0; n < n_steps; ++n) {
-    SQG_CUDA(cudaGraphLaunch(pl->graph_exec, st));
+    SQG_CUDA(cudaGraphLaunch(pl->graph_exec, cs));
     pl->launches += 8;
   }
+  SQG_CUDA(cudaEventRecord(pl->ev_out, cs));
+  SQG_CUDA(cudaStreamWaitEvent(st, pl->ev_out, 0));
+  SQG_CUDA(cudaMemcpyAsync(theta, state, full, cudaMemcpyDeviceToDevice, st));
   return SQG_OK;
 }
 

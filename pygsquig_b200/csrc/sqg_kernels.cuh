@@ -421,6 +421,14 @@ k_row(KP kp, RowArgs a) {
 // ---------------------------------------------------------------------------
 // Column pass
 // ---------------------------------------------------------------------------
+// Device-side control of the ring phases for CUDA-graph replays: the phases
+// of step n are base + n * n_ring; the column pass of stage 4 advances ctr.
+struct RingCtl {
+  const double* base;
+  int ctr;
+  int pad;
+};
+
 enum ColMode { CM_THETA = 0, CM_SCAL = 1, CM_VEL = 2, CM_PHYS1 = 3, CM_FWD = 4 };
 
 struct ColArgs {
@@ -436,6 +444,7 @@ struct ColArgs {
   int stage;
   const void* ring_theta;   // theta_s (full spectrum) the rate is measured on
   const double* phases;     // n_ring phases of this step
+  RingCtl* ctl;             // if set, phases = ctl->base + ctl->ctr * n_ring
   const int* ring_pos;      // n_ring flat indices ix*N+iy
   const int* ring_mirror;   // ordinal of -k for each ring mode
   double2* ringF;           // [4][n_ring] out
@@ -622,10 +631,11 @@ __device__ void ring_reduce(const KP& kp, const ColArgs& a) {
   const int n = kp.n_ring;
   const int s = a.stage;
   double2* F = a.ringF + (size_t)(s - 1) * n;
+  const double* phases = a.ctl ? a.ctl->base + (size_t)a.ctl->ctr * n : a.phases;
   // 1. raw forcing of this stage
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     double sn, cs;
-    sincos(a.phases[i], &sn, &cs);
+    sincos(phases[i], &sn, &cs);
     double2 f = make_double2(a.ring_amp * cs, a.ring_amp * sn);
     if (a.ring_ou) {
       if (*a.ou_init) {
@@ -639,6 +649,7 @@ __device__ void ring_reduce(const KP& kp, const ColArgs& a) {
   __syncthreads();
   if (threadIdx.x == 0) {
     if (a.ring_ou) *a.ou_init = 1;
+    if (a.ctl && s == 4) a.ctl->ctr += 1;  // every thread has read this step's phases
     for (int h = 0; h < 4; ++h) {
       const int o = a.herm_ord[h];
       if (o >= 0) F[o].y = 0.0;
@@ -680,4 +691,11 @@ __device__ void ring_reduce(const KP& kp, const ColArgs& a) {
   }
 }
 
+}  // namespace sqg
+
+namespace sqg {
+__global__ void k_set_ctl(RingCtl* ctl, const double* base) {
+  ctl->base = base;
+  ctl->ctr = 0;
+}
 }  // namespace sqg
