@@ -103,6 +103,24 @@ int sqg_ring_modes(const sqg_plan* plan, int32_t* ix, int32_t* iy);
  * (replaces _compute_core_rhs, pygsquig/core/solver.py:28-58). */
 int sqg_rhs(sqg_plan* plan, const void* theta_hat, void* rhs, void* stream);
 
+/* No counterpart in the reference.  sqg_rhs for callers that cannot
+ * allocate device memory -- for example a host application that reserves all
+ * device memory up front through its own allocator, or a latency-critical loop
+ * in which cudaMalloc/cudaFree are not allowed because they can synchronise
+ * the device.  It takes a descriptor instead of a plan and needs no
+ * workspace: the grid tables and intermediate fields live in a static device
+ * array of SQG_NOALLOC_SCRATCH_BYTES (3 MiB) that every GPU loading the
+ * library keeps until the process exits.  Limit: N <= SQG_NOALLOC_MAX_N (256),
+ * larger N is rejected with SQG_ERR_INVALID.  The first call on a device
+ * resolves the array's device address (cudaGetSymbolAddress) for that
+ * device; make that first call before any stream capture.  Every call
+ * rewrites the whole array, so calls that overlap on the GPU (other streams,
+ * other host threads) race and must be serialised by the caller.  Only N, L,
+ * alpha, nu_p, p and precision of the descriptor are used. */
+#define SQG_NOALLOC_MAX_N 256
+#define SQG_NOALLOC_SCRATCH_BYTES (3u << 20)
+int sqg_rhs_noalloc(const sqg_desc* desc, const void* theta_hat, void* rhs, void* stream);
+
 /* One RK4 step theta_out = step(theta_in) (replaces gSQGSolver.step with the
  * plan's forcing/damping, solver.py:182-214 + time_integrator.py:14-36).
  * ring_phases: device float64[n_ring] in [0, 2pi) (NULL if no ring forcing).

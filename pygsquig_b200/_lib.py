@@ -64,6 +64,7 @@ SIGNATURES = {
     "sqg_ring_mode_count": [_vp, C.POINTER(_i32)],
     "sqg_ring_modes": [_vp, C.POINTER(_i32), C.POINTER(_i32)],
     "sqg_rhs": [_vp, _vp, _vp, _vp],
+    "sqg_rhs_noalloc": [C.POINTER(SqgDesc), _vp, _vp, _vp],
     "sqg_step": [_vp, _vp, _vp, _dbl, _vp, _vp],
     "sqg_multistep": [_vp, _vp, _i32, _dbl, _vp, _i32, _vp],
     "sqg_stage_begin": [_vp, _vp, _vp],

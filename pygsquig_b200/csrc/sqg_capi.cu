@@ -1008,3 +1008,148 @@ int sqg_last_launch_count(const sqg_plan* pl, int64_t* n) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// sqg_rhs_noalloc: the core RHS for callers that cannot allocate device memory.
+//
+// Some host programs must not call cudaMalloc from the code that calls this
+// library -- e.g. a coupler or plugin host that reserves all device memory up
+// front through its own allocator, or a latency-critical loop where
+// cudaMalloc/cudaFree are banned because they can synchronise the device.
+// Such a caller passes only its input and output spectra.  Everything else
+// (grid tables and the intermediate transformed fields) lives in the
+// file-scope array below, which every GPU that loads this library holds for
+// the life of the process.
+// ---------------------------------------------------------------------------
+namespace {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SQG_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+void* g_noalloc_dev_ptr[kMaxDevices] = {};  // device address of g_noalloc_scratch, per device
+
+// Grid tables of the no-allocation path, computed on the device with the
+// same float64 expressions the host path uses (round-to-nearest intrinsics
+// keep the compiler from contracting them into FMAs, so the dealiasing mask
+// edges are the reference's bit for bit).
+template <typename T>
+__global__ void k_noalloc_tables(int N, double L, double* k1d, T* k1t, typename Cplx<T>::type* tw, RowTab* rows,
+                                 unsigned* status) {
+  using C = typename Cplx<T>::type;
+  const int H = N / 2;
+  const double dx = __ddiv_rn(L, (double)N);
+  const double val = __ddiv_rn(1.0, __dmul_rn((double)N, dx));
+  const int npos = (N - 1) / 2 + 1;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const double m = i < npos ? (double)i : (double)(i - N);
+    const double k = __dmul_rn(__dmul_rn(__dmul_rn(m, val), 2.0), M_PI);
+    k1d[i] = k;
+    k1t[i] = (T)k;
+    double sn, cs;
+    sincospi(2.0 * i / N, &sn, &cs);
+    tw[i] = mkc<C>(cs, -sn);
+  }
+  __syncthreads();
+  const double cutoff = __dmul_rn(2.0 / 3.0, __ddiv_rn(__dmul_rn(M_PI, (double)N), L));
+  for (int ix = threadIdx.x; ix < N; ix += blockDim.x) {
+    const double kx2 = __dmul_rn(k1d[ix], k1d[ix]);
+    RowTab rt;
+    rt.dmax = -1;
+    rt.dragmax = -1;
+    for (int my = 0; my <= H; ++my) {
+      const double ky = k1d[my];
+      if (__dsqrt_rn(__dadd_rn(kx2, __dmul_rn(ky, ky))) < cutoff) rt.dmax = my;
+    }
+    rt.pos_lo = 1; rt.pos_hi = 0; rt.neg_lo = 1; rt.neg_hi = 0;
+    rt.row_start = 0;
+    rt.pad = 0;
+    rows[ix] = rt;
+  }
+  if (threadIdx.x == 0) *status = 0u;
+}
+
+template <typename T>
+cudaError_t noalloc_tables(int N, double L, unsigned char* base, size_t o_k1d, size_t o_k1t, size_t o_tw,
+                           size_t o_rows, size_t o_status, cudaStream_t st) {
+  k_noalloc_tables<T><<<1, 256, 0, st>>>(N, L, (double*)(base + o_k1d), (T*)(base + o_k1t),
+                                         (typename Cplx<T>::type*)(base + o_tw), (RowTab*)(base + o_rows),
+                                         (unsigned*)(base + o_status));
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" int sqg_rhs_noalloc(const sqg_desc* desc, const void* theta, void* rhs, void* stream) {
+  if (!desc || !theta || !rhs) return fail(SQG_ERR_INVALID, "null argument");
+  const sqg_desc& d = *desc;
+  int log2n = 0;
+  while ((1 << log2n) < d.N) ++log2n;
+  if ((1 << log2n) != d.N || d.N < 8 || d.N > SQG_NOALLOC_MAX_N)
+    return fail(SQG_ERR_INVALID, "sqg_rhs_noalloc: N must be a power of two in [8, " +
+                                     std::to_string(SQG_NOALLOC_MAX_N) + "] (static scratch of " +
+                                     std::to_string(SQG_NOALLOC_SCRATCH_BYTES >> 20) + " MiB), got " +
+                                     std::to_string(d.N));
+  if (!(d.alpha >= -2 && d.alpha <= 2)) return fail(SQG_ERR_INVALID, "alpha must be in [-2, 2], got " + std::to_string(d.alpha));
+  if (d.p != 2 && d.p != 4 && d.p != 8) return fail(SQG_ERR_INVALID, "p must be 2, 4, or 8, got " + std::to_string(d.p));
+  if (d.precision != SQG_F64 && d.precision != SQG_F32) return fail(SQG_ERR_INVALID, "bad precision");
+  if (!(d.L > 0)) return fail(SQG_ERR_INVALID, "L must be positive");
+  int dev = 0;
+  SQG_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(SQG_ERR_INVALID, "device index out of range");
+  // One-time set-up per device (the current one): the device address of the
+  // static array.  In host code the array's name is only a host-side stand-in.
+  if (!g_noalloc_dev_ptr[dev]) {
+    void* p = nullptr;
+    SQG_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_dev_ptr[dev] = p;
+  }
+  // A plan that lives on the stack and points into the static scratch.
+  sqg_plan pl;
+  pl.d = d;
+  pl.d.has_damping = 0;
+  pl.d.has_ring = 0;
+  pl.d.n_scalars = 0;
+  pl.N = d.N;
+  pl.H = d.N / 2;
+  pl.log2N = log2n;
+  pl.csize = d.precision == SQG_F64 ? 16 : 8;
+  pl.akind = alpha_kind(d.alpha);
+  const size_t N = d.N, cs = pl.csize, half = (N / 2 + 1) * N * cs;
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t r = o; o += align256(bytes); return r; };
+  pl.off_k1d = take(N * sizeof(double));
+  pl.off_k1t = take(N * cs / 2);
+  pl.off_tw = take(N * cs);
+  pl.off_rows = take(N * sizeof(RowTab));
+  pl.off_status = take(sizeof(unsigned));
+  pl.off_ringF = pl.off_status;
+  pl.off_xh = take(4 * half);
+  pl.off_jh = take(half);
+  pl.off_acc = pl.off_stage = pl.off_xh;  // unused by the RHS passes
+  if (o > SQG_NOALLOC_SCRATCH_BYTES) return fail(SQG_ERR_INVALID, "sqg_rhs_noalloc: scratch too small");
+  pl.ws = (unsigned char*)g_noalloc_dev_ptr[dev];
+  pl.ws_bytes = SQG_NOALLOC_SCRATCH_BYTES;
+  pl.ready = true;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (d.precision == SQG_F64) {
+    SQG_CUDA(noalloc_tables<double>(pl.N, d.L, pl.ws, pl.off_k1d, pl.off_k1t, pl.off_tw, pl.off_rows, pl.off_status, st));
+    SQG_CUDA(set_attrs_p<double>(log2n));
+  } else {
+    SQG_CUDA(noalloc_tables<float>(pl.N, d.L, pl.ws, pl.off_k1d, pl.off_k1t, pl.off_tw, pl.off_rows, pl.off_status, st));
+    SQG_CUDA(set_attrs_p<float>(log2n));
+  }
+  int rc = run_p1(&pl, theta, FM_THETA, nullptr, st);
+  if (rc != SQG_OK) return rc;
+  KP kp = make_kp(&pl, 0.0);
+  kp.ring_on = 0;
+  ColArgs ca = base_col(&pl);
+  SQG_CUDA(launch_col(&pl, kp, ca, st));
+  RowArgs ra = base_row(&pl);
+  ra.rmode = RM_RHS;
+  ra.stage = 1;
+  ra.th_n = theta;
+  ra.rhs_out = rhs;
+  ra.do_p1 = 0;
+  SQG_CUDA(launch_row(&pl, kp, ra, st));
+  return SQG_OK;
+}
