@@ -15,6 +15,7 @@ One "step" = one RK4 step of the field; metric = RK4 steps/s.
 "hires4096": gSQG alpha = 0.5 at N = 4096, ring kf=100, dk=2, eps=0.1,
 mu=0.05, nu=1e-20, p=8, dt=5e-5, k^-3 initial field (seed 3), plus two
 passive scalars (kappa = 1e-4) with mean-gradient forcing G = (1, 0).
+"forced4096": the same without the scalars (the theta step alone).
 
 Timing: CUDA events on the launching stream; each timed step is bracketed by
 its own events and the L2 cache is flushed (a 256 MiB write) between steps
@@ -43,6 +44,8 @@ WORKLOADS = {
                        ic="k4exp", ic_seed=2, noise_seed=1, scalars=0),
     "hires4096": dict(N=4096, alpha=0.5, kf=100.0, dk=2.0, eps=0.1, mu=0.05, kf_damp=100.0, nu=1e-20, p=8, dt=5e-5,
                       ic="kminus3", ic_seed=3, noise_seed=4, scalars=2),
+    "forced4096": dict(N=4096, alpha=0.5, kf=100.0, dk=2.0, eps=0.1, mu=0.05, kf_damp=100.0, nu=1e-20, p=8, dt=5e-5,
+                       ic="kminus3", ic_seed=3, noise_seed=4, scalars=0),
 }
 
 
@@ -155,7 +158,7 @@ def ncu_traffic(workload, prec, kernel):
     return d.get(f"{workload}/{prec}/{kernel}")
 
 
-def cpu_baseline(w, seconds=12.0, warm=1):
+def cpu_baseline(w, seconds=12.0, warm=None):
     """The float64 CPU restatement of the reference algorithm (9 complex
     FFTs per RHS, forcing rescale with 2 more), IF-RK4, scipy.fft threads =
     all host cores; a bounded number of steps."""
@@ -170,6 +173,8 @@ def cpu_baseline(w, seconds=12.0, warm=1):
     st = s.initialize(theta0=initial_field(O, g, w))
     rng = np.random.default_rng(w["noise_seed"])
     n_ring = O.ring_mode_count(g, w["kf"], w["dk"])
+    if warm is None:
+        warm = 1 if w["N"] <= 1024 else 0
     for _ in range(warm):
         st = O.step_forced(s, st, w["dt"], ring, rng.uniform(0, 2 * np.pi, n_ring), damp)
     n, t0 = 0, time.perf_counter()

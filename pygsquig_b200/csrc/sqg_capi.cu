@@ -241,39 +241,89 @@ KP make_kp(const sqg_plan* pl, double dt) {
 }
 
 // ---- compile-time launch shapes ----
-constexpr int rows_per_cta(int log2n) { return (1 << log2n) / 8 >= 128 ? 1 : 128 / ((1 << log2n) / 8); }
-constexpr int pairs_per_cta(int log2n) {
-  return ((1 << log2n) / 8 >= 256) ? 1
-         : (256 / ((1 << log2n) / 8) > 16 ? ((1 << log2n) / 2 < 16 ? (1 << log2n) / 2 : 16)
-                                          : 256 / ((1 << log2n) / 8));
+// Radix of the group FFTs.  Column pass: 16 for float grids with N >= 1024
+// (groups of N/16 threads, fewer barrier rounds, two blocks per SM); row
+// pass: 8 (each thread walks R elements of the stage update).
+template <typename T, int L>
+constexpr int col_radix() { return 8; }
+template <typename T, int L>
+constexpr int row_radix() { return 8; }
+template <typename T, int L>
+constexpr int row_group() { return (1 << L) / row_radix<T, L>(); }
+template <typename T, int L>
+constexpr int col_group() { return (1 << L) / col_radix<T, L>(); }
+template <typename T, int L>
+constexpr int rows_per_cta() { return row_group<T, L>() >= 128 ? 1 : 128 / row_group<T, L>(); }
+template <typename T, int L>
+constexpr int pairs_per_cta() {
+  constexpr int g = col_group<T, L>();
+  constexpr int cap = (1 << L) / 2 < 16 ? (1 << L) / 2 : 16;
+  return g >= 256 ? 1 : (256 / g > cap ? cap : 256 / g);
+}
+// Four resident field buffers per column pair when they fit in 150 KB.
+template <typename T, int L>
+constexpr int col_nbuf() {
+  return (size_t)pairs_per_cta<T, L>() * 4 * ColBuf<(1 << L), col_radix<T, L>()>::SZ *
+                     sizeof(typename Cplx<T>::type) <= 150 * 1024 ? 4 : 2;
+}
+// Exchange buffers of the row pass: four (the theta fields transform
+// together) when they fit in 150 KB, else two (two rounds).
+template <typename T, int L>
+constexpr int row_nfx() {
+  return (size_t)rows_per_cta<T, L>() * 4 * spad_size<row_radix<T, L>()>(1 << L) * sizeof(typename Cplx<T>::type) <=
+                 150 * 1024 ? 4 : 2;
+}
+template <typename T, int L>
+constexpr size_t row_base_smem() {
+  return (size_t)rows_per_cta<T, L>() * row_nfx<T, L>() * spad_size<row_radix<T, L>()>(1 << L) *
+         sizeof(typename Cplx<T>::type);
+}
+template <typename T, int L>
+constexpr size_t row_pf_bytes(int depth) {
+  return (size_t)rows_per_cta<T, L>() * depth * 4 * row_group<T, L>() * sizeof(typename Cplx<T>::type);
+}
+// Prefetch depth of the row pass: all R chunks when the block fits the budget
+// (220 KB when registers allow one block per SM anyway, else 110 KB), else
+// the largest power of two that fits.
+template <typename T, int L>
+constexpr int row_depth() {
+  constexpr size_t budget = rows_per_cta<T, L>() * row_group<T, L>() >= 512 ? 220 * 1024 : 110 * 1024;
+  constexpr int R = row_radix<T, L>();
+  return row_base_smem<T, L>() + row_pf_bytes<T, L>(R) <= budget       ? R
+         : row_base_smem<T, L>() + row_pf_bytes<T, L>(R / 2) <= budget ? R / 2
+         : row_base_smem<T, L>() + row_pf_bytes<T, L>(R / 4) <= budget ? R / 4
+                                                                       : 1;
+}
+template <typename T, int L>
+size_t row_smem() { return row_base_smem<T, L>() + row_pf_bytes<T, L>(row_depth<T, L>()); }
+template <typename T, int L>
+size_t col_smem() {
+  return (size_t)pairs_per_cta<T, L>() * col_nbuf<T, L>() * ColBuf<(1 << L), col_radix<T, L>()>::SZ *
+         sizeof(typename Cplx<T>::type);
 }
 
 template <typename T, int L>
-size_t row_smem() { return (size_t)rows_per_cta(L) * 2 * (1 << L) * sizeof(typename Cplx<T>::type); }
-template <typename T, int L>
-size_t col_smem() { return (size_t)pairs_per_cta(L) * 2 * (1 << L) * sizeof(typename Cplx<T>::type); }
-
-template <typename T, int L>
 cudaError_t launch_row_t(const KP& kp, const RowArgs& a, cudaStream_t st) {
-  constexpr int N = 1 << L, RPC = rows_per_cta(L), G = N / 8;
+  constexpr int N = 1 << L, RPC = rows_per_cta<T, L>();
   const int grid = (N / 2 + 1 + RPC - 1) / RPC;
-  k_row<T, L, RPC><<<grid, RPC * G, row_smem<T, L>(), st>>>(kp, a);
+  k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()><<<grid, RPC * row_group<T, L>(), row_smem<T, L>(), st>>>(kp, a);
   return cudaGetLastError();
 }
 template <typename T, int L>
 cudaError_t launch_col_t(const KP& kp, const ColArgs& a, cudaStream_t st, bool ring_only) {
-  constexpr int N = 1 << L, NP = pairs_per_cta(L), G = N / 8;
+  constexpr int N = 1 << L, NP = pairs_per_cta<T, L>();
   int grid = ring_only ? 1 : N / (2 * NP) + (a.ring_cta ? 1 : 0);
-  k_col<T, L, NP><<<grid, NP * G, col_smem<T, L>(), st>>>(kp, a);
+  k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()><<<grid, NP * col_group<T, L>(), col_smem<T, L>(), st>>>(kp, a);
   return cudaGetLastError();
 }
 template <typename T, int L>
 cudaError_t set_attrs_t() {
-  constexpr int RPC = rows_per_cta(L), NP = pairs_per_cta(L);
-  cudaError_t e = cudaFuncSetAttribute(k_row<T, L, RPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)row_smem<T, L>());
+  constexpr int RPC = rows_per_cta<T, L>(), NP = pairs_per_cta<T, L>();
+  cudaError_t e = cudaFuncSetAttribute(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem<T, L>());
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_col<T, L, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem<T, L>());
+  return cudaFuncSetAttribute(k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem<T, L>());
 }
 
 #define SQG_DISPATCH(LOG2N, FN, ...)                  \

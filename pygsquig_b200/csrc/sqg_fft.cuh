@@ -20,6 +20,13 @@ template <typename T> struct Cplx;
 template <> struct Cplx<float> { using type = float2; };
 template <> struct Cplx<double> { using type = double2; };
 
+// Shared-memory index of element i in an exchange buffer of a radix-R
+// transform: one padding slot every R elements makes the Stockham store
+// patterns (strides R and R^2 in elements) and the strided loads bank-conflict
+// free.  A padded buffer of N elements occupies spad_size<R>(N) = N + N/R slots.
+template <int R> __device__ __forceinline__ int spad(int i) { return i + (i >> (R == 16 ? 4 : 3)); }
+template <int R> __host__ __device__ constexpr int spad_size(int n) { return n + n / R; }
+
 template <typename C> __device__ __forceinline__ C mkc(double x, double y) {
   C r; r.x = x; r.y = y; return r;
 }
@@ -57,11 +64,11 @@ __device__ __forceinline__ void dft4(C& a0, C& a1, C& a2, C& a3) {
   a1 = cadd(d02, d13); a3 = csub(d02, d13);
 }
 
-// In-place 8-point DFT with sign DIR of v[0..7] (natural order in and out).
+// In-place DFTs with sign DIR of v[o + s*r], r = 0..n-1 (natural order).
 template <int DIR, typename T, typename C>
-__device__ __forceinline__ void dft8(C (&v)[8]) {
-  C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
-  C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+__device__ __forceinline__ void dft8s(C* v, int o, int st) {
+  C e0 = v[o], e1 = v[o + 2 * st], e2 = v[o + 4 * st], e3 = v[o + 6 * st];
+  C o0 = v[o + st], o1 = v[o + 3 * st], o2 = v[o + 5 * st], o3 = v[o + 7 * st];
   dft4<DIR>(e0, e1, e2, e3);
   dft4<DIR>(o0, o1, o2, o3);
   const T r = (T)0.70710678118654752440;  // 1/sqrt(2)
@@ -71,77 +78,162 @@ __device__ __forceinline__ void dft8(C (&v)[8]) {
   C t2 = mul_i<DIR>(o2);
   // o3 * (-1 + DIR i)/sqrt2
   t3.x = (-o3.x - (T)DIR * o3.y) * r; t3.y = (-o3.y + (T)DIR * o3.x) * r;
-  v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
-  v[1] = cadd(e1, t1); v[5] = csub(e1, t1);
-  v[2] = cadd(e2, t2); v[6] = csub(e2, t2);
-  v[3] = cadd(e3, t3); v[7] = csub(e3, t3);
+  v[o] = cadd(e0, o0); v[o + 4 * st] = csub(e0, o0);
+  v[o + st] = cadd(e1, t1); v[o + 5 * st] = csub(e1, t1);
+  v[o + 2 * st] = cadd(e2, t2); v[o + 6 * st] = csub(e2, t2);
+  v[o + 3 * st] = cadd(e3, t3); v[o + 7 * st] = csub(e3, t3);
 }
 
-// Group FFT.  v: this thread's eight values in strided layout (in and out).
-// sbuf: N complex values of shared memory private to the group.  All
-// threads of the block must call it together (it uses __syncthreads).
-// On entry sbuf may still be read by other threads of the block only if the
-// caller synchronises first; the routine begins with a barrier before its
-// first write.  On exit other threads may still be reading sbuf: callers
-// synchronise before writing to it again.
-template <typename T, int LOG2N, int DIR>
-__device__ __forceinline__ void fft_group(typename Cplx<T>::type (&v)[8],
-                                          typename Cplx<T>::type* sbuf, int j,
-                                          const typename Cplx<T>::type* __restrict__ tw) {
+// 16-point DFT as 4 x 4: DFT4 over the stride-4 subsequences, twiddles
+// exp(DIR 2 pi i k m / 16), DFT4 across, transposed write-back.
+template <int DIR, typename T, typename C>
+__device__ __forceinline__ void dft16(C (&v)[16]) {
+  const T c1 = (T)0.92387953251128675613;  // cos(pi/8)
+  const T s1 = (T)0.38268343236508977173;  // sin(pi/8)
+  const T h = (T)0.70710678118654752440;   // cos(pi/4)
+#pragma unroll
+  for (int k = 0; k < 4; ++k) dft4<DIR>(v[k], v[k + 4], v[k + 8], v[k + 12]);
+  // v[k + 4 m] now holds X_k[m]; multiply by w16^(k m), w16 = exp(DIR 2 pi i / 16)
+  auto rot = [&](C a, T c, T s) {  // a * (c + DIR i s)
+    C r;
+    r.x = a.x * c - (T)DIR * a.y * s;
+    r.y = a.y * c + (T)DIR * a.x * s;
+    return r;
+  };
+  v[5] = rot(v[5], c1, s1);    // k=1 m=1: w^1
+  v[9] = rot(v[9], h, h);      // k=1 m=2: w^2
+  v[13] = rot(v[13], s1, c1);  // k=1 m=3: w^3
+  v[6] = rot(v[6], h, h);      // k=2 m=1: w^2
+  v[10] = mul_i<DIR>(v[10]);   // k=2 m=2: w^4
+  v[14] = rot(v[14], -h, h);   // k=2 m=3: w^6
+  v[7] = rot(v[7], s1, c1);    // k=3 m=1: w^3
+  v[11] = rot(v[11], -h, h);   // k=3 m=2: w^6
+  v[15] = rot(v[15], -c1, -s1);  // k=3 m=3: w^9
+#pragma unroll
+  for (int m = 0; m < 4; ++m) dft4<DIR>(v[4 * m], v[4 * m + 1], v[4 * m + 2], v[4 * m + 3]);
+  // v[4 m + n] holds X[m + 4 n]; transpose to natural order
+  C t[16];
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int n = 0; n < 4; ++n) t[m + 4 * n] = v[4 * m + n];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = t[i];
+}
+
+// NF independent group FFTs executed together.  v[f]: this thread's R
+// values of transform f in strided layout, v[f][m] = x_f[j + m G] with
+// G = N/R (in and out).  sbuf + f * bstride: spad_size<R>(N) complex slots of
+// shared memory for transform f (indexed through spad<R>).  The NF
+// transforms share every barrier and every twiddle load, which gives each
+// thread NF times the independent work per pass.  All threads of the block
+// must call it together (it uses __syncthreads).  The routine begins with a
+// barrier before its first write to sbuf; on exit other threads may still be
+// reading sbuf, so callers synchronise before writing to it again.  Passes:
+// one pass of radix 2^(log2 N mod log2 R) first when log2 N is not a multiple
+// of log2 R (each thread then runs R / that radix butterflies), then radix-R
+// passes.
+template <typename T, int LOG2N, int R, int DIR, int NF>
+__device__ __forceinline__ void fft_multi(typename Cplx<T>::type (&v)[NF][R], typename Cplx<T>::type* sbuf,
+                                          int bstride, int j, const typename Cplx<T>::type* __restrict__ tw) {
   using C = typename Cplx<T>::type;
+  constexpr int LR = R == 16 ? 4 : 3;
   constexpr int N = 1 << LOG2N;
-  constexpr int G = N / 8;
-  constexpr int REM = LOG2N % 3;
-  constexpr int NP8 = LOG2N / 3;
+  constexpr int G = N / R;
+  constexpr int REM = LOG2N % LR;
+  constexpr int NPR = LOG2N / LR;
   constexpr bool INV = DIR > 0;
-  static_assert(LOG2N >= 3, "N >= 8");
+  static_assert(R == 8 || R == 16, "radix 8 or 16");
+  static_assert(LOG2N >= LR, "N >= R");
   int p = 1;
   if (REM != 0) {
     constexpr int RP = 1 << REM;
-    constexpr int NB = 8 / RP;
+    constexpr int NB = R / RP;
 #pragma unroll
-    for (int q = 0; q < NB; ++q) {
-      if (RP == 2) {
-        dft2<DIR>(v[q], v[q + NB]);
-      } else {
-        dft4<DIR>(v[q], v[q + NB], v[q + 2 * NB], v[q + 3 * NB]);
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        if (RP == 2) {
+          dft2<DIR>(v[f][q], v[f][q + NB]);
+        } else if (RP == 4) {
+          dft4<DIR>(v[f][q], v[f][q + NB], v[f][q + 2 * NB], v[f][q + 3 * NB]);
+        } else {
+          dft8s<DIR, T>(v[f], q, NB);
+        }
       }
-    }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < NB; ++q) {
-      const int i = j + q * G;  // butterfly index, p = 1 so k = 0
+    for (int f = 0; f < NF; ++f)
 #pragma unroll
-      for (int r = 0; r < RP; ++r) sbuf[i * RP + r] = v[q + r * NB];
-    }
+      for (int q = 0; q < NB; ++q) {
+        const int i = j + q * G;  // butterfly index, p = 1 so k = 0
+#pragma unroll
+        for (int r = 0; r < RP; ++r) sbuf[f * bstride + spad<R>(i * RP + r)] = v[f][q + r * NB];
+      }
     __syncthreads();
 #pragma unroll
-    for (int m = 0; m < 8; ++m) v[m] = sbuf[j + m * G];
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int m = 0; m < R; ++m) v[f][m] = sbuf[f * bstride + spad<R>(j + m * G)];
     p = RP;
   }
-#pragma unroll
-  for (int pass = 0; pass < NP8; ++pass) {
+  // Radix-R passes.  The pass loop is kept rolled so that its code is shared
+  // by all passes (the unrolled form overflows the instruction cache).
+  int lp = REM;  // log2(p)
+#pragma unroll 1
+  for (int pass = 0; pass < NPR; ++pass) {
     const int k = j & (p - 1);
     if (p > 1) {
-      const int stride = N / (p * 8);
+      // w^r for r = 1..R-1 from one table load w = exp(-+2 pi i k / (p R)):
+      // powers by complex products (at most three chained roundings)
+      const C w1 = tw[(k << (LOG2N - lp - LR)) & (N - 1)];
+      C wp[R];
+      wp[1] = w1;
+      wp[2] = cmul(w1, w1);
+      wp[3] = cmul(wp[2], w1);
+      wp[4] = cmul(wp[2], wp[2]);
+      wp[5] = cmul(wp[4], w1);
+      wp[6] = cmul(wp[3], wp[3]);
+      wp[7] = cmul(wp[4], wp[3]);
+      if constexpr (R == 16) {
+        wp[8] = cmul(wp[4], wp[4]);
 #pragma unroll
-      for (int r = 1; r < 8; ++r) {
-        const C w = tw[(r * k * stride) & (N - 1)];
-        v[r] = cmul_tw<INV>(v[r], w);
+        for (int r = 9; r < 16; ++r) wp[r] = cmul(wp[8], wp[r - 8]);
       }
-    }
-    dft8<DIR, T>(v);
-    if (pass != NP8 - 1) {
-      __syncthreads();
-      const int base = (j - k) * 8 + k;
 #pragma unroll
-      for (int r = 0; r < 8; ++r) sbuf[base + r * p] = v[r];
+      for (int r = 1; r < R; ++r)
+#pragma unroll
+        for (int f = 0; f < NF; ++f) v[f][r] = cmul_tw<INV>(v[f][r], wp[r]);
+    }
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      if constexpr (R == 16) dft16<DIR, T>(v[f]);
+      else dft8s<DIR, T>(v[f], 0, 1);
+    }
+    if (pass != NPR - 1) {
+      __syncthreads();
+      const int base = (j - k) * R + k;
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int r = 0; r < R; ++r) sbuf[f * bstride + spad<R>(base + r * p)] = v[f][r];
       __syncthreads();
 #pragma unroll
-      for (int m = 0; m < 8; ++m) v[m] = sbuf[j + m * G];
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int m = 0; m < R; ++m) v[f][m] = sbuf[f * bstride + spad<R>(j + m * G)];
     }
-    p *= 8;
+    p *= R;
+    lp += LR;
   }
+}
+
+// One group FFT (see fft_multi).
+template <typename T, int LOG2N, int R, int DIR>
+__device__ __forceinline__ void fft_group(typename Cplx<T>::type (&v)[R], typename Cplx<T>::type* sbuf, int j,
+                                          const typename Cplx<T>::type* __restrict__ tw) {
+  using C = typename Cplx<T>::type;
+  fft_multi<T, LOG2N, R, DIR, 1>(*reinterpret_cast<C(*)[1][R]>(&v), sbuf, 0, j, tw);
 }
 
 }  // namespace sqg

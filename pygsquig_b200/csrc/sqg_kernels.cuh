@@ -87,6 +87,26 @@ struct RowArgs {
   double gx[4], gy[4];
 };
 
+// ---- asynchronous global -> shared copies (cp.async) ----
+__device__ __forceinline__ void cp_async_elem(void* smem, const void* gmem, int bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if (bytes == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int NPENDING>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(NPENDING) : "memory"); }
+
+// Resident blocks per SM the register allocation must allow: at most 128
+// registers per thread in float, about 168 in double.
+template <typename T>
+constexpr int min_blocks(int threads) {
+  return sizeof(T) == 4 ? (65536 / (threads * 128) > 8 ? 8 : (65536 / (threads * 128) > 0 ? 65536 / (threads * 128) : 1))
+                        : (65536 / (threads * 168) > 8 ? 8 : (65536 / (threads * 168) > 0 ? 65536 / (threads * 168) : 1));
+}
+
 __device__ __forceinline__ int mode_abs(int i, int N) { return i <= (N >> 1) ? i : N - i; }
 
 // |k|^-alpha with k = 0 -> 0 (operators.py:134-155)
@@ -126,19 +146,108 @@ __device__ __forceinline__ int ring_ord(const RowTab& rt, int iy) {
 // ---------------------------------------------------------------------------
 // Row pass
 // ---------------------------------------------------------------------------
-template <typename T, int LOG2N, int RPC>
-__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / 8))
+// Field kinds of the inverse transforms along y: spectrum X of
+//   u: -i m (dky H + nky A)   v: i m (dkx H + nkx A)   (m = |k|^-alpha)
+//   dx: i dkx H   dy: i dky H   id: H,   all times 1/N^2,
+// where H / A are the Hermitian / anti-Hermitian parts of theta at (k, -k),
+// dk = k except 0 on the Nyquist index and nk = k only on the Nyquist index
+// (the reference's .real projections, operators.py:15-34, 76-97, 101-130).
+enum FieldKind { FK_U = 0, FK_V = 1, FK_DX = 2, FK_DY = 3, FK_ID = 4 };
+
+__device__ __forceinline__ int field_kind(int fmode, int f) {
+  if (fmode == FM_THETA || fmode == FM_VEL) return f;  // u, v, dx, dy
+  if (fmode == FM_PHYS1) return FK_ID;
+  return FK_DX + f;                                    // scalar: dx, dy
+}
+
+// Fields f0 .. f0+NF-1 of the row pair's mode: form their spectra from
+// theta_{s+1} at (p, iy) / (N-p, N-iy), transform them together along y and
+// write xh[f][p][:].  Also writes the mean-gradient source spectra of the
+// scalars when asked (needs u and v in the same batch).
+template <typename T, int LOG2N, int R, int NF>
+__device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, const typename Cplx<T>::type (&t1)[R],
+                                           const typename Cplx<T>::type (&t2)[R], int f0, int j, int p, bool valid,
+                                           typename Cplx<T>::type* wbuf) {
+  using C = typename Cplx<T>::type;
+  constexpr int N = 1 << LOG2N, G = N / R, H = N / 2, XB = spad_size<R>(N);
+  const T* __restrict__ k1t = reinterpret_cast<const T*>(kp.k1t);
+  const C* __restrict__ tw = reinterpret_cast<const C*>(kp.tw);
+  const T kx = k1t[p];
+  const T s_n2 = (T)kp.inv_n2;
+  const T dkx = (p == H) ? (T)0 : kx;
+  const T nkx = (p == H) ? kx : (T)0;
+  const bool uv = (a.fmode == FM_THETA || a.fmode == FM_VEL);
+  C V[NF][R];
+#pragma unroll
+  for (int m = 0; m < R; ++m) {
+    const int iy = j + m * G;
+    const C h = cscale(cadd(t1[m], cconj(t2[m])), (T)0.5);
+    const C an = cscale(csub(t1[m], cconj(t2[m])), (T)0.5);
+    const T ky = k1t[iy];
+    const T dky = (iy == H) ? (T)0 : ky;
+    const T nky = (iy == H) ? ky : (T)0;
+    T mm = (T)0;
+    if (uv) mm = inv_frac<T>(kx * kx + ky * ky, (T)kp.alpha, kp.akind) * s_n2;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      const int kind = field_kind(a.fmode, f0 + f);
+      C X;
+      if (kind == FK_U) {
+        const C q = cadd(cscale(h, dky), cscale(an, nky));
+        X = mkc<C>(mm * q.y, -mm * q.x);
+      } else if (kind == FK_V) {
+        const C q = cadd(cscale(h, dkx), cscale(an, nkx));
+        X = mkc<C>(-mm * q.y, mm * q.x);
+      } else if (kind == FK_DX) {
+        X = mkc<C>(-dkx * s_n2 * h.y, dkx * s_n2 * h.x);
+      } else if (kind == FK_DY) {
+        X = mkc<C>(-dky * s_n2 * h.y, dky * s_n2 * h.x);
+      } else {
+        X = cscale(h, s_n2);
+      }
+      V[f][m] = X;
+    }
+    if (NF >= 2 && uv && f0 == 0 && a.n_src > 0 && valid) {
+      // S^ = -N^2 (gx X_u + gy X_v): the mean-gradient scalar source
+      const T n2 = (T)1 / s_n2;
+      for (int sidx = 0; sidx < a.n_src; ++sidx) {
+        C* so = reinterpret_cast<C*>(a.src_out[sidx]);
+        const T gx = (T)a.gx[sidx], gy = (T)a.gy[sidx];
+        so[(size_t)p * N + iy] =
+            mkc<C>(-n2 * (gx * V[0][m].x + gy * V[1][m].x), -n2 * (gx * V[0][m].y + gy * V[1][m].y));
+      }
+    }
+  }
+  fft_multi<T, LOG2N, R, +1, NF>(V, wbuf, XB, j, tw);
+  if (valid) {
+    C* xh = reinterpret_cast<C*>(a.xh);
+    const size_t fstride = (size_t)(H + 1) * N;
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int m = 0; m < R; ++m) xh[(f0 + f) * fstride + (size_t)p * N + j + m * G] = V[f][m];
+  }
+}
+
+// Row pass.  DEPTH: how many of the R element chunks of a thread (chunk m =
+// the elements iy = j + m G) have their theta_n / acc values prefetched with
+// cp.async ahead of use; the first DEPTH chunks are requested before the
+// forward FFT of the J row, so their latency hides behind it.
+template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
+__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), min_blocks<T>(RPC * ((1 << LOG2N) / R)))
 k_row(KP kp, RowArgs a) {
   using C = typename Cplx<T>::type;
   constexpr int N = 1 << LOG2N;
-  constexpr int G = N / 8;
+  constexpr int G = N / R;
   constexpr int H = N / 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* smem = reinterpret_cast<C*>(smem_raw);
   const int grp = threadIdx.x / G;
   const int j = threadIdx.x - grp * G;
-  C* hbuf = smem + grp * (2 * N);
-  C* wbuf = hbuf + N;
+  constexpr int XB = spad_size<R>(N);  // one exchange buffer
+  C* wbuf = smem + (size_t)grp * NFX * XB;  // NFX exchange buffers of this group
+  // prefetch staging: DEPTH chunks x 4 slots (theta_n e1/e2, acc e1/e2) x G
+  C* pf = smem + (size_t)RPC * NFX * XB + (size_t)grp * (DEPTH * 4 * G);
   const int p_raw = blockIdx.x * RPC + grp;
   const bool valid = p_raw <= H;
   const int p = valid ? p_raw : H;
@@ -152,32 +261,54 @@ k_row(KP kp, RowArgs a) {
   const T s_n2 = (T)kp.inv_n2;
   bool bad = false;
 
-  C v[8];   // FFT registers
-  C t1[8];  // theta_{s+1} (or theta_in) at e1 = (p, iy)
-  C t2[8];  // theta_{s+1} at e2 = (pp, N - iy)
+  C v[R];   // FFT registers
+  C t1[R];  // theta_{s+1} (or theta_in) at e1 = (p, iy)
+  C t2[R];  // theta_{s+1} at e2 = (pp, N - iy)
 
   if (a.rmode == RM_P1) {
     const C* th = reinterpret_cast<const C*>(a.th_n);
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
+    for (int m = 0; m < R; ++m) {
       const int iy = j + m * G;
       const int iyp = (N - iy) & (N - 1);
       t1[m] = th[(size_t)p * N + iy];
       t2[m] = th[(size_t)pp * N + iyp];
     }
   } else {
+    // stage pass: request this thread's theta_n / acc elements of the first
+    // DEPTH chunks (own slots only, so no barrier is needed to consume them)
+    const bool pf_th = a.rmode == RM_STAGE && a.stage <= 3;
+    const bool pf_acc = a.rmode == RM_STAGE && a.stage >= 2;
+    const C* pth = reinterpret_cast<const C*>(a.th_n);
+    const C* pacc = reinterpret_cast<const C*>(a.acc);
+    auto issue = [&](int m) {
+      const int iy = j + m * G;
+      const int iyp = (N - iy) & (N - 1);
+      C* slot = pf + (size_t)(m % DEPTH) * 4 * G + j;
+      if (pf_th) {
+        cp_async_elem(slot, pth + (size_t)p * N + iy, (int)sizeof(C));
+        if (pair) cp_async_elem(slot + G, pth + (size_t)pp * N + iyp, (int)sizeof(C));
+      }
+      if (pf_acc) {
+        cp_async_elem(slot + 2 * G, pacc + (size_t)p * N + iy, (int)sizeof(C));
+        if (pair) cp_async_elem(slot + 3 * G, pacc + (size_t)pp * N + iyp, (int)sizeof(C));
+      }
+      cp_async_commit();
+    };
+#pragma unroll
+    for (int m = 0; m < DEPTH; ++m) issue(m);
     // forward DFT along y of the x-transformed Jacobian row p
     const C* jh = reinterpret_cast<const C*>(a.jh);
 #pragma unroll
-    for (int m = 0; m < 8; ++m) v[m] = jh[(size_t)p * N + j + m * G];
-    fft_group<T, LOG2N, -1>(v, wbuf, j, tw);
+    for (int m = 0; m < R; ++m) v[m] = jh[(size_t)p * N + j + m * G];
+    fft_group<T, LOG2N, R, -1>(v, wbuf, j, tw);
     // v[m] = J^(p, iy) ; J^(pp, N - iy) = conj(v[m])
     if (a.rmode == RM_SPEC) {
       // forward transform of a real field: rows p and N - p of its spectrum
       C* out = reinterpret_cast<C*>(a.rhs_out);
       if (valid) {
 #pragma unroll
-        for (int m = 0; m < 8; ++m) {
+        for (int m = 0; m < R; ++m) {
           const int iy = j + m * G;
           out[(size_t)p * N + iy] = v[m];
           if (pair) out[(size_t)pp * N + ((N - iy) & (N - 1))] = cconj(v[m]);
@@ -197,12 +328,14 @@ k_row(KP kp, RowArgs a) {
     const double dt = kp.dt;
     const bool explicit_lin = (kp.scheme == 0);
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
+    for (int m = 0; m < R; ++m) {
       const int iy = j + m * G;
       const int iyp = (N - iy) & (N - 1);
       const size_t e1 = (size_t)p * N + iy;
       const size_t e2 = (size_t)pp * N + iyp;
       const int my = mode_abs(iy, N);
+      cp_async_wait<DEPTH - 1>();  // chunk m has landed (groups are issued in order)
+      const C* slot = pf + (size_t)(m % DEPTH) * 4 * G + j;
       const double kyd = kp.k1d[iy];
       const double k2d = kxd * kxd + kyd * kyd;
       // diagonal linear operator in float64
@@ -251,11 +384,16 @@ k_row(KP kp, RowArgs a) {
           const C x2 = st_in[e2];
           if (valid) out[e2] = cadd(n2, cscale(x2, Ls));
         }
+        if (m + DEPTH < R) issue(m + DEPTH);
+        else cp_async_commit();
         continue;
       }
       C k1v = n1, k2v = n2;
       C xs1 = mkc<C>(0, 0), xs2 = mkc<C>(0, 0);  // stage input
-      if (explicit_lin || s == 1) {
+      if (s == 1) {
+        xs1 = slot[0];
+        if (pair) xs2 = slot[G];
+      } else if (explicit_lin) {
         xs1 = st_in[e1];
         if (pair) xs2 = st_in[e2];
       }
@@ -283,26 +421,26 @@ k_row(KP kp, RowArgs a) {
           o2 = cscale(cadd(xs2, cscale(k2v, tdt * (T)0.5)), E);
         }
       } else if (s == 2 || s == 3) {
-        C a1 = acc[e1];
+        C a1 = slot[2 * G];
         a1 = cadd(a1, cscale(k1v, tdt / (T)3 * E));
         if (valid) acc[e1] = a1;
-        const C x1 = th_n[e1];
+        const C x1 = slot[0];
         if (s == 2) o1 = cadd(cscale(x1, E), cscale(k1v, tdt * (T)0.5));   // th3 = E th + dt/2 k
         else        o1 = cadd(cscale(x1, E2), cscale(k1v, tdt * E));       // th4 = E^2 th + dt E k
         if (pair) {
-          C a2 = acc[e2];
+          C a2 = slot[3 * G];
           a2 = cadd(a2, cscale(k2v, tdt / (T)3 * E));
           if (valid) acc[e2] = a2;
-          const C x2 = th_n[e2];
+          const C x2 = slot[G];
           if (s == 2) o2 = cadd(cscale(x2, E), cscale(k2v, tdt * (T)0.5));
           else        o2 = cadd(cscale(x2, E2), cscale(k2v, tdt * E));
         }
       } else {
         // th_{n+1} = acc + dt/6 k
-        o1 = cadd(acc[e1], cscale(k1v, tdt / (T)6));
+        o1 = cadd(slot[2 * G], cscale(k1v, tdt / (T)6));
         if (valid) th_out[e1] = o1;
         if (pair) {
-          o2 = cadd(acc[e2], cscale(k2v, tdt / (T)6));
+          o2 = cadd(slot[3 * G], cscale(k2v, tdt / (T)6));
           if (valid) th_out[e2] = o2;
         }
       }
@@ -315,6 +453,8 @@ k_row(KP kp, RowArgs a) {
       bad |= !(cfinite(o1) && cfinite(o2));
       t1[m] = o1;
       t2[m] = o2;
+      if (m + DEPTH < R) issue(m + DEPTH);
+      else cp_async_commit();  // empty group keeps the in-order accounting
     }
   }
   if (kp.status) {
@@ -328,93 +468,26 @@ k_row(KP kp, RowArgs a) {
     __syncthreads();
     if (!pair) {
 #pragma unroll
-      for (int m = 0; m < 8; ++m) hbuf[j + m * G] = t1[m];
+      for (int m = 0; m < R; ++m) wbuf[j + m * G] = t1[m];
     }
     __syncthreads();
     if (!pair) {
 #pragma unroll
-      for (int m = 0; m < 8; ++m) t2[m] = hbuf[(N - (j + m * G)) & (N - 1)];
+      for (int m = 0; m < R; ++m) t2[m] = wbuf[(N - (j + m * G)) & (N - 1)];
     }
-    __syncthreads();
   }
-
-  // ---- inverse transforms along y of the multiplied Hermitian projections ----
-  C* xh = reinterpret_cast<C*>(a.xh);
-  const size_t fstride = (size_t)(H + 1) * N;
-  const bool theta_like = (a.fmode == FM_THETA || a.fmode == FM_VEL);
-  const T dkx = (p == H) ? (T)0 : kx;
-  const T nkx = (p == H) ? kx : (T)0;
-  C a_nyq = mkc<C>(0, 0);
-  // first field straight from registers
-#pragma unroll
-  for (int m = 0; m < 8; ++m) {
-    const int iy = j + m * G;
-    const C h = cscale(cadd(t1[m], cconj(t2[m])), (T)0.5);
-    const C an = cscale(csub(t1[m], cconj(t2[m])), (T)0.5);
-    hbuf[j + m * G] = h;
-    if (iy == H) a_nyq = an;
-    const T ky = k1t[iy];
-    const T dky = (iy == H) ? (T)0 : ky;
-    C X;
-    if (theta_like) {
-      const T k2 = kx * kx + ky * ky;
-      const T mm = inv_frac<T>(k2, (T)kp.alpha, kp.akind) * s_n2;
-      // v: i m (dkx H + nkx A)
-      C q = cadd(cscale(h, dkx), cscale(an, nkx));
-      X = mkc<C>(-mm * q.y, mm * q.x);
-      if (a.n_src > 0 && valid) {
-        // u: -i m (dky H + nky A); S^ = -N^2 (gx X_u + gy X_v)
-        const T nky = (iy == H) ? ky : (T)0;
-        C qu = cadd(cscale(h, dky), cscale(an, nky));
-        C Xu = mkc<C>(mm * qu.y, -mm * qu.x);
-        const T n2 = (T)1 / s_n2;
-        for (int sidx = 0; sidx < a.n_src; ++sidx) {
-          C* so = reinterpret_cast<C*>(a.src_out[sidx]);
-          const T gx = (T)a.gx[sidx], gy = (T)a.gy[sidx];
-          so[(size_t)p * N + iy] = mkc<C>(-n2 * (gx * Xu.x + gy * X.x), -n2 * (gx * Xu.y + gy * X.y));
-        }
-      }
-    } else if (a.fmode == FM_PHYS1) {
-      X = cscale(h, s_n2);
-    } else {  // FM_SCAL: s_x = i dkx H
-      X = mkc<C>(-dkx * s_n2 * h.y, dkx * s_n2 * h.x);
+  // Inverse transforms along y of the multiplied Hermitian projections.
+  if (a.fmode == FM_THETA) {
+    if (NFX >= 4) {
+      row_fields<T, LOG2N, R, 4>(kp, a, t1, t2, 0, j, p, valid, wbuf);
+    } else {
+      row_fields<T, LOG2N, R, 2>(kp, a, t1, t2, 0, j, p, valid, wbuf);
+      row_fields<T, LOG2N, R, 2>(kp, a, t1, t2, 2, j, p, valid, wbuf);
     }
-    v[m] = X;
-  }
-  const int f_first = theta_like ? 1 : 0;
-  fft_group<T, LOG2N, +1>(v, wbuf, j, tw);
-  if (valid) {
-#pragma unroll
-    for (int m = 0; m < 8; ++m) xh[f_first * fstride + (size_t)p * N + j + m * G] = v[m];
-  }
-  int nf = (a.fmode == FM_THETA) ? 4 : (a.fmode == FM_PHYS1 ? 1 : 2);
-  for (int f = 0; f < nf; ++f) {
-    if (f == f_first) continue;
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      const int iy = j + m * G;
-      const C h = hbuf[j + m * G];
-      const T ky = k1t[iy];
-      const T dky = (iy == H) ? (T)0 : ky;
-      C X;
-      if (theta_like && f == 0) {
-        const T k2 = kx * kx + ky * ky;
-        const T mm = inv_frac<T>(k2, (T)kp.alpha, kp.akind) * s_n2;
-        const T nky = (iy == H) ? ky : (T)0;
-        C q = cadd(cscale(h, dky), cscale(a_nyq, nky));
-        X = mkc<C>(mm * q.y, -mm * q.x);
-      } else if ((a.fmode == FM_THETA && f == 2)) {
-        X = mkc<C>(-dkx * s_n2 * h.y, dkx * s_n2 * h.x);
-      } else {  // theta_y or s_y: i dky H
-        X = mkc<C>(-dky * s_n2 * h.y, dky * s_n2 * h.x);
-      }
-      v[m] = X;
-    }
-    fft_group<T, LOG2N, +1>(v, wbuf, j, tw);
-    if (valid) {
-#pragma unroll
-      for (int m = 0; m < 8; ++m) xh[f * fstride + (size_t)p * N + j + m * G] = v[m];
-    }
+  } else if (a.fmode == FM_PHYS1) {
+    row_fields<T, LOG2N, R, 1>(kp, a, t1, t2, 0, j, p, valid, wbuf);
+  } else {
+    row_fields<T, LOG2N, R, 2>(kp, a, t1, t2, 0, j, p, valid, wbuf);
   }
 }
 
@@ -456,40 +529,60 @@ struct ColArgs {
   double* ring_scale_out;   // [4]
 };
 
-// Complete a half column of a field pair into shared memory:
-// Z(kx) = xa + i xb (kx <= N/2), Z(N - kx) = conj(xa) + i conj(xb).
-template <typename T>
-__device__ __forceinline__ void col_load_pair(const typename Cplx<T>::type* __restrict__ f, int N, int y0,
-                                              int npair, typename Cplx<T>::type* smem) {
+// Slots of one field buffer of a column group: the raw half columns
+// A[kx] = x(kx, ya) at slot kx and B[kx] = x(kx, ya + 1) at slot H + 1 + kx
+// (kx = 0..N/2), later reused as the padded FFT exchange buffer.
+template <int N, int R> struct ColBuf { static constexpr int SZ = spad_size<R>(N) + 2; };
+
+// Issue the copies of the half columns of field f for every column pair of
+// the block into buffer slot `buf` of each group (no registers, no wait).
+template <typename T, int LOG2N, int R, int NP, int NBUF>
+__device__ __forceinline__ void col_fetch(const typename Cplx<T>::type* __restrict__ f, int y0, int buf,
+                                          typename Cplx<T>::type* smem) {
   using C = typename Cplx<T>::type;
-  const int H = N / 2;
-  const int total = (H + 1) * npair;
-  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    const int kx = idx / npair;
-    const int q = idx - kx * npair;
-    const int ya = y0 + 2 * q;
-    const C xa = f[(size_t)kx * N + ya];
-    const C xb = f[(size_t)kx * N + ya + 1];
-    C* z = smem + (size_t)q * (2 * N);
-    if (kx == 0 || kx == H) {
-      z[kx] = mkc<C>(xa.x, xb.x);
-    } else {
-      z[kx] = mkc<C>(xa.x - xb.y, xa.y + xb.x);
-      z[N - kx] = mkc<C>(xa.x + xb.y, -xa.y + xb.x);
-    }
+  constexpr int N = 1 << LOG2N, H = N / 2, G = N / R, NT = NP * G, SZ = ColBuf<N, R>::SZ;
+  constexpr int TOTAL = (H + 1) * NP * 2;
+  for (int idx = threadIdx.x; idx < TOTAL; idx += NT) {
+    const int c = idx % (2 * NP);      // column within the block (fastest: coalesced rows)
+    const int kx = idx / (2 * NP);
+    const int q = c >> 1, b = c & 1;
+    C* z = smem + (size_t)(q * NBUF + buf) * SZ;
+    cp_async_elem(z + b * (H + 1) + kx, f + (size_t)kx * N + y0 + c, (int)sizeof(C));
+  }
+}
+
+// First-pass load of a packed column pair: Z(x) = xa + i xb completed to a
+// Hermitian column (Z(N - kx) = conj xa + i conj xb), from the raw slots.
+template <typename T, int LOG2N, int R>
+__device__ __forceinline__ void col_first_load(const typename Cplx<T>::type* z, int j,
+                                               typename Cplx<T>::type (&v)[R]) {
+  using C = typename Cplx<T>::type;
+  constexpr int N = 1 << LOG2N, H = N / 2, G = N / R;
+#pragma unroll
+  for (int m = 0; m < R; ++m) {
+    const int x = j + m * G;
+    const int kx = x <= H ? x : N - x;
+    const C xa = z[kx], xb = z[H + 1 + kx];
+    if (x == 0 || x == H) v[m] = mkc<C>(xa.x, xb.x);
+    else if (x < H) v[m] = mkc<C>(xa.x - xb.y, xa.y + xb.x);
+    else v[m] = mkc<C>(xa.x + xb.y, -xa.y + xb.x);
   }
 }
 
 template <typename T, int LOG2N>
 __device__ void ring_reduce(const KP& kp, const ColArgs& a);
 
-template <typename T, int LOG2N, int NP>
-__global__ void __launch_bounds__(NP * ((1 << LOG2N) / 8))
+// Column pass.  NBUF = 4: all four fields of the column pairs are fetched at
+// once (round-2 copies land while round 1 computes); NBUF = 2: two rounds of
+// two fields (large N in float64, where four buffers do not fit).
+template <typename T, int LOG2N, int R, int NP, int NBUF>
+__global__ void __launch_bounds__(NP * ((1 << LOG2N) / R), min_blocks<T>(NP * ((1 << LOG2N) / R)))
 k_col(KP kp, ColArgs a) {
   using C = typename Cplx<T>::type;
   constexpr int N = 1 << LOG2N;
-  constexpr int G = N / 8;
+  constexpr int G = N / R;
   constexpr int H = N / 2;
+  constexpr int SZ = ColBuf<N, R>::SZ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* smem = reinterpret_cast<C*>(smem_raw);
   if (a.ring_cta && blockIdx.x == gridDim.x - 1) {
@@ -498,40 +591,37 @@ k_col(KP kp, ColArgs a) {
   }
   const int grp = threadIdx.x / G;
   const int j = threadIdx.x - grp * G;
-  C* bufA = smem + grp * (2 * N);
-  C* bufB = bufA + N;
+  C* gbuf = smem + (size_t)grp * NBUF * SZ;  // this group's NBUF buffers
   const int y0 = blockIdx.x * (2 * NP);
   const int ya = y0 + 2 * grp;
   const C* __restrict__ tw = reinterpret_cast<const C*>(kp.tw);
   const C* xh = reinterpret_cast<const C*>(a.xh);
   const size_t fstride = (size_t)(H + 1) * N;
-  C v[8];
+  C v[R];
 
   if (a.cmode == CM_VEL || a.cmode == CM_PHYS1) {
     const int nf = a.cmode == CM_VEL ? 2 : 1;
-    // field 0 -> bufA, field 1 -> bufB
-    col_load_pair<T>(xh, N, y0, NP, smem);
-    if (nf == 2) col_load_pair<T>(xh + fstride, N, y0, NP, smem + N);
+    for (int f = 0; f < nf; ++f) col_fetch<T, LOG2N, R, NP, NBUF>(xh + f * fstride, y0, f, smem);
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();
     for (int f = 0; f < nf; ++f) {
-      C* b = f == 0 ? bufA : bufB;
-#pragma unroll
-      for (int m = 0; m < 8; ++m) v[m] = b[j + m * G];
-      fft_group<T, LOG2N, +1>(v, b, j, tw);
+      C* b = gbuf + f * SZ;
+      col_first_load<T, LOG2N, R>(b, j, v);
+      fft_group<T, LOG2N, R, +1>(v, b, j, tw);
       // v[m] = f(x, ya) + i f(x, ya+1), x = j + m G
       if (a.cmode == CM_PHYS1 || a.out1) {
         T* o = reinterpret_cast<T*>(f == 0 ? a.out0 : a.out1);
 #pragma unroll
-        for (int m = 0; m < 8; ++m) {
+        for (int m = 0; m < R; ++m) {
           const size_t x = j + m * G;
           o[x * N + ya] = v[m].x;
           o[x * N + ya + 1] = v[m].y;
         }
       } else {
-        // complex u + i v output
-        T* o = reinterpret_cast<T*>(a.out0);
+        T* o = reinterpret_cast<T*>(a.out0);  // complex u + i v output
 #pragma unroll
-        for (int m = 0; m < 8; ++m) {
+        for (int m = 0; m < R; ++m) {
           const size_t x = j + m * G;
           o[2 * (x * N + ya) + f] = v[m].x;
           o[2 * (x * N + ya + 1) + f] = v[m].y;
@@ -541,62 +631,84 @@ k_col(KP kp, ColArgs a) {
     return;
   }
 
-  // CM_THETA: rounds (u, theta_x), (v, theta_y); CM_SCAL: one round (s_x, s_y)
-  C W[8];
+  // CM_THETA: the four fields (u, theta_x, v, theta_y) transformed together
+  // (NBUF = 4) or in two rounds of two (NBUF = 2); CM_SCAL: one round
+  // (s_x, s_y) with (u, v) read from global; CM_FWD: forward transform only.
+  C W[R];
 #pragma unroll
-  for (int m = 0; m < 8; ++m) W[m] = mkc<C>(0, 0);
+  for (int m = 0; m < R; ++m) W[m] = mkc<C>(0, 0);
+  const int nround = a.cmode == CM_THETA ? 2 : (a.cmode == CM_SCAL ? 1 : 0);
+  const int fa0 = 0, fb0 = a.cmode == CM_THETA ? 2 : 1, fa1 = 1, fb1 = 3;
+  if (nround > 0) {
+    col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa0 * fstride, y0, 0, smem);
+    col_fetch<T, LOG2N, R, NP, NBUF>(xh + fb0 * fstride, y0, 1, smem);
+    if (NBUF == 4 && nround == 2) {
+      col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa1 * fstride, y0, 2, smem);
+      col_fetch<T, LOG2N, R, NP, NBUF>(xh + fb1 * fstride, y0, 3, smem);
+    }
+    cp_async_commit();
+  }
   if (a.cmode == CM_FWD) {
     const T* f = reinterpret_cast<const T*>(a.in_real);
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
+    for (int m = 0; m < R; ++m) {
       const size_t x = j + m * G;
       W[m] = mkc<C>(f[x * N + ya], f[x * N + ya + 1]);
     }
   }
-  const int nround = a.cmode == CM_THETA ? 2 : (a.cmode == CM_SCAL ? 1 : 0);
-  for (int rd = 0; rd < nround; ++rd) {
-    if (rd) __syncthreads();
-    const int fa = (a.cmode == CM_THETA) ? (rd == 0 ? 0 : 1) : 0;
-    const int fb = (a.cmode == CM_THETA) ? (rd == 0 ? 2 : 3) : 1;
-    col_load_pair<T>(xh + fa * fstride, N, y0, NP, smem);
-    col_load_pair<T>(xh + fb * fstride, N, y0, NP, smem + N);
+  if (NBUF == 4 && nround == 2) {
+    cp_async_wait<0>();
     __syncthreads();
+    C V[4][R];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) v[m] = bufA[j + m * G];
-    fft_group<T, LOG2N, +1>(v, bufA, j, tw);
-    __syncthreads();
+    for (int f = 0; f < 4; ++f) col_first_load<T, LOG2N, R>(gbuf + f * SZ, j, V[f]);
+    fft_multi<T, LOG2N, R, +1, 4>(V, gbuf, SZ, j, tw);
+    // J = u theta_x + v theta_y for columns a (real parts) and b (imaginary)
 #pragma unroll
-    for (int m = 0; m < 8; ++m) bufA[j + m * G] = v[m];  // velocity-like field, own slots
-#pragma unroll
-    for (int m = 0; m < 8; ++m) v[m] = bufB[j + m * G];
-    fft_group<T, LOG2N, +1>(v, bufB, j, tw);
-    if (a.cmode == CM_THETA) {
-      // W += (ua * txa) + i (ub * txb)
-#pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const C u = bufA[j + m * G];
-        W[m].x += u.x * v[m].x;
-        W[m].y += u.y * v[m].y;
+    for (int m = 0; m < R; ++m) {
+      W[m].x = V[0][m].x * V[1][m].x + V[2][m].x * V[3][m].x;
+      W[m].y = V[0][m].y * V[1][m].y + V[2][m].y * V[3][m].y;
+    }
+  } else {
+    for (int rd = 0; rd < nround; ++rd) {
+      if (rd == 1) {
+        __syncthreads();  // round-1 buffers free
+        col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa1 * fstride, y0, 0, smem);
+        col_fetch<T, LOG2N, R, NP, NBUF>(xh + fb1 * fstride, y0, 1, smem);
+        cp_async_commit();
       }
-    } else {
-      // bufA: s_x(a) + i s_x(b); v: s_y(a) + i s_y(b); uv from global
-      const C* uv = reinterpret_cast<const C*>(a.uv);
+      cp_async_wait<0>();
+      __syncthreads();
+      C V[2][R];
+      col_first_load<T, LOG2N, R>(gbuf, j, V[0]);
+      col_first_load<T, LOG2N, R>(gbuf + SZ, j, V[1]);
+      fft_multi<T, LOG2N, R, +1, 2>(V, gbuf, SZ, j, tw);
+      if (a.cmode == CM_THETA) {
 #pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const size_t x = j + m * G;
-        const C sx = bufA[j + m * G];
-        const C w0 = uv[x * N + ya];
-        const C w1 = uv[x * N + ya + 1];
-        W[m].x = w0.x * sx.x + w0.y * v[m].x;
-        W[m].y = w1.x * sx.y + w1.y * v[m].y;
+        for (int m = 0; m < R; ++m) {
+          W[m].x += V[0][m].x * V[1][m].x;
+          W[m].y += V[0][m].y * V[1][m].y;
+        }
+      } else {
+        // V0: s_x(a) + i s_x(b); V1: s_y(a) + i s_y(b); (u, v) from global
+        const C* uvp = reinterpret_cast<const C*>(a.uv);
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+          const size_t x = j + m * G;
+          const C w0 = uvp[x * N + ya];
+          const C w1 = uvp[x * N + ya + 1];
+          W[m].x = w0.x * V[0][m].x + w0.y * V[1][m].x;
+          W[m].y = w1.x * V[0][m].y + w1.y * V[1][m].y;
+        }
       }
     }
   }
   // forward DFT along x of Ja + i Jb
-  fft_group<T, LOG2N, -1>(W, bufA, j, tw);
+  C* bufX = gbuf;
+  fft_group<T, LOG2N, R, -1>(W, bufX, j, tw);
   __syncthreads();
 #pragma unroll
-  for (int m = 0; m < 8; ++m) bufA[j + m * G] = W[m];
+  for (int m = 0; m < R; ++m) bufX[spad<R>(j + m * G)] = W[m];
   __syncthreads();
   // split: Ja(kx) = (W(kx) + conj W(-kx))/2, Jb(kx) = -i (W(kx) - conj W(-kx))/2
   C* jh = reinterpret_cast<C*>(a.jh);
@@ -604,9 +716,9 @@ k_col(KP kp, ColArgs a) {
   for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
     const int kx = idx / NP;
     const int q = idx - kx * NP;
-    const C* w = smem + (size_t)q * (2 * N);
-    const C wk = w[kx];
-    const C wm = w[(N - kx) & (N - 1)];
+    const C* w = smem + (size_t)q * NBUF * SZ;
+    const C wk = w[spad<R>(kx)];
+    const C wm = w[spad<R>((N - kx) & (N - 1))];
     const C ja = mkc<C>((T)0.5 * (wk.x + wm.x), (T)0.5 * (wk.y - wm.y));
     const C d = mkc<C>(wk.x - wm.x, wk.y + wm.y);
     const C jb = mkc<C>((T)0.5 * d.y, (T)-0.5 * d.x);
