@@ -55,6 +55,34 @@ def initial_field(O, g, w):
     return O.random_phase_field(g, lambda k: k ** (-3.0), w["ic_seed"])
 
 
+def ensemble_members(O, seed=7):
+    """96 realisations: 48 x 128^2, 32 x 256^2, 16 x 512^2; alpha uniform in
+    {0, 0.5, 1, 1.5}; 0-3 passive scalars (kappa 1e-4, Gaussian blobs of
+    width 0.3 at seeded centres); theta random-phase with a spectrum peaked at
+    k0 = 8, rms 1."""
+    from pygsquig_b200.ensemble import Member
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for N, count in ((128, 48), (256, 32), (512, 16)):
+        g = O.make_grid(N, 2 * np.pi)
+        x = np.arange(N) * 2 * np.pi / N
+        X, Y = np.meshgrid(x, x, indexing="ij")
+        for _ in range(count):
+            alpha = float(rng.choice([0.0, 0.5, 1.0, 1.5]))
+            th0 = O.random_phase_field(g, lambda k: (k / 8.0) ** 4 * np.exp(-2 * (k / 8.0) ** 2),
+                                       int(rng.integers(1 << 30)))
+            ns = int(rng.integers(0, 4))
+            sc = []
+            for _ in range(ns):
+                cx, cy = rng.uniform(0, 2 * np.pi, 2)
+                dx = np.angle(np.exp(1j * (X - cx)))
+                dy = np.angle(np.exp(1j * (Y - cy)))
+                sc.append(np.exp(-(dx**2 + dy**2) / (2 * 0.3**2)))
+            out.append(Member(N, alpha, th0, sc, [1e-4] * ns))
+    return out
+
+
 def bytes_per_launch(N, w_bytes):
     """Algorithmic bytes of each pass per launch (model stated in DESIGN.md).
 
@@ -235,12 +263,12 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="forced1024", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="forced1024", choices=sorted(WORKLOADS) + ["ensemble96"])
     ap.add_argument("--precision", default="float32", choices=["float32", "float64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="auto", help="extra measured variants: auto|none")
     args = ap.parse_args()
-    w = WORKLOADS[args.workload]
+    w = WORKLOADS.get(args.workload, WORKLOADS["forced1024"])
     if args.impl == "reference":
         return run_reference(args, w)
     args.warmup = max(args.warmup, 3)
@@ -372,6 +400,50 @@ def main():
         del flush
         return res
 
+    def measure_ensemble(steps, warmup):
+        """Config-3 ensemble: every member advanced by graph-replayed multistep."""
+        from pygsquig_b200.ensemble import EnsembleSolver
+
+        members = ensemble_members(O)
+        ens = EnsembleSolver(members, nu_p=1e-6, p=8, precision="float32", scheme="ifrk4")
+        ens.multistep(warmup, 5e-4)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stream = torch.cuda.current_stream()
+        e0.record(stream)
+        ens.multistep(steps, 5e-4)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        finite = all(bool(torch.isfinite(torch.view_as_real(t)).all().item()) for t in ens.theta)
+        n_scal = sum(len(m.scalars0) for m in members)
+        return {"value": world * steps / (ms / 1e3), "unit": "ensemble steps/s",
+                "member_steps_per_s": world * len(members) * steps / (ms / 1e3), "ms_per_step": ms / steps,
+                "members": len(members), "passive_scalars": n_scal, "steps": steps, "finite": finite,
+                "gpu_launches_per_step": ens.launches_per_step(),
+                "config": "48x128^2 + 32x256^2 + 16x512^2, alpha in {0,.5,1,1.5}, 0-3 scalars, FP32 IF-RK4, "
+                          "nu=1e-6 p=8 dt=5e-4, one CUDA graph per size class per step, no L2 flush "
+                          "(working set > L2)"}
+
+    if args.workload == "ensemble96":
+        r = measure_ensemble(args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps({"metric": "RK4 ensemble steps/s", "value": r["value"], "unit": r["unit"], "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                              "data": "synthetic", "config": {"workload": "ensemble96", "detail": r["config"]},
+                              "ensemble": r}))
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+
     peak, peak_kind = measured_peaks()
     prec = args.precision
     main_res = measure(args.workload, prec, args.steps, args.warmup, True, True)
@@ -424,6 +496,8 @@ def main():
                                     "ms_per_step": v["ms"] / v["steps"], "finite": v["finite"],
                                     "kernels": {k: {"launches": c, "avg_us": 1e3 * m / max(c, 1)}
                                                 for k, (m, c) in v["kernels"].items() if c}}
+    if args.variants == "auto":
+        line["variant_ensemble96"] = measure_ensemble(200, 10)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

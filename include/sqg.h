@@ -194,6 +194,31 @@ int sqg_scalar_variance(sqg_plan* plan, const void* s_hat, double* out, void* st
 int sqg_scalars_step(sqg_plan* plan, const void* theta_new, const void* const* scalars_in,
                      void* const* scalars_out, double dt, void* stream);
 
+/* Batched ensembles (replaces the pmap ensemble of multi_gpu.py:118-155 on
+ * one GPU): members share N, precision, scheme and the solver/damping
+ * physics of the descriptor; alpha and up to SQG_MAX_SCALARS passive scalars
+ * (diffusivity kappa, no source) vary per member.  Every pass of an RK stage
+ * is one launch over all members (member = blockIdx.y); sqg_batch_multistep
+ * advances every member's state in place, replaying one captured CUDA graph
+ * per step.  Each step updates theta first, then the member's scalars with
+ * theta's new velocity frozen over the stages (solver_with_scalars.py:
+ * 131-178).  Ring forcing is not carried by batches. */
+typedef struct sqg_member {
+  void* theta;                       /* N x N spectrum, advanced in place */
+  double alpha;
+  int32_t n_scalars;
+  int32_t reserved;
+  void* scalars[SQG_MAX_SCALARS];    /* N x N spectra, advanced in place */
+  double kappa[SQG_MAX_SCALARS];
+} sqg_member;
+typedef struct sqg_batch sqg_batch;
+int sqg_batch_create(const sqg_desc* desc, int32_t n_members, const sqg_member* members, sqg_batch** out);
+int sqg_batch_workspace_bytes(const sqg_batch* batch, size_t* bytes);
+int sqg_batch_set_workspace(sqg_batch* batch, void* workspace, size_t bytes, void* stream);
+int sqg_batch_multistep(sqg_batch* batch, int32_t n_steps, double dt, int32_t use_graph, void* stream);
+int sqg_batch_last_launch_count(const sqg_batch* batch, int64_t* launches);
+int sqg_batch_destroy(sqg_batch* batch);
+
 /* Reads and clears the sticky status flags (bit 0: non-finite value seen).
  * Synchronises the stream. */
 int sqg_check_status(sqg_plan* plan, uint32_t* flags, void* stream);

@@ -53,6 +53,17 @@ class SqgDesc(C.Structure):
     ]
 
 
+class SqgMember(C.Structure):
+    _fields_ = [
+        ("theta", C.c_void_p),
+        ("alpha", C.c_double),
+        ("n_scalars", C.c_int32),
+        ("reserved", C.c_int32),
+        ("scalars", C.c_void_p * SQG_MAX_SCALARS),
+        ("kappa", C.c_double * SQG_MAX_SCALARS),
+    ]
+
+
 # Every symbol include/sqg.h declares, with its argument types.
 _vp, _i32, _dbl, _sz = C.c_void_p, C.c_int32, C.c_double, C.c_size_t
 SIGNATURES = {
@@ -85,6 +96,12 @@ SIGNATURES = {
     "sqg_plan_host_tables": [_vp, _vp, _vp, _vp],
     "sqg_set_timing": [_vp, _i32],
     "sqg_timing_read": [_vp, _vp, _vp, _i32],
+    "sqg_batch_create": [C.POINTER(SqgDesc), _i32, C.POINTER(SqgMember), C.POINTER(C.c_void_p)],
+    "sqg_batch_workspace_bytes": [_vp, C.POINTER(_sz)],
+    "sqg_batch_set_workspace": [_vp, _vp, _sz, _vp],
+    "sqg_batch_multistep": [_vp, _i32, _dbl, _i32, _vp],
+    "sqg_batch_last_launch_count": [_vp, C.POINTER(C.c_int64)],
+    "sqg_batch_destroy": [_vp],
     "sqg_last_error_string": [],
     "sqg_version": [],
 }

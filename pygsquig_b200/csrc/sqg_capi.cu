@@ -1203,3 +1203,383 @@ extern "C" int sqg_rhs_noalloc(const sqg_desc* desc, const void* theta, void* rh
   SQG_CUDA(launch_row(&pl, kp, ra, st));
   return SQG_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Batched ensembles: every member of a batch has the same N and precision
+// (one size class); alpha and the passive scalars vary per member.  One
+// launch advances all members through a pass (member = blockIdx.y); a whole
+// ensemble step is captured once in a CUDA graph and replayed.
+// ---------------------------------------------------------------------------
+struct sqg_batch {
+  sqg_desc d;  // common physics: N, precision, scheme, p, nu_p, L, damping
+  int N, H, log2N, M, S;
+  size_t csize;
+  std::vector<sqg_member> mem;
+  std::vector<int> scal_member, scal_slot;  // scalar batch entry -> (member, slot)
+  sqg_plan tables;                           // grid tables (a plan without per-field buffers)
+  unsigned char* ws = nullptr;
+  size_t ws_bytes = 0, off_tab = 0, off_member = 0, member_stride = 0, off_scalar = 0, scalar_stride = 0,
+         off_args = 0, off_total = 0;
+  // offsets inside a member block / scalar block
+  size_t m_acc, m_stage, m_xh, m_jh, m_uv, s_acc, s_stage, s_xs, s_js;
+  // device argument arrays
+  KP* d_kp = nullptr;            // [M]
+  KP* d_kps = nullptr;           // [S]
+  RowArgs* d_p1 = nullptr;       // [M]
+  ColArgs* d_col = nullptr;      // [M]
+  RowArgs* d_row = nullptr;      // [4][M]
+  ColArgs* d_vel = nullptr;      // [M]
+  RowArgs* d_sp1 = nullptr;      // [S]
+  ColArgs* d_scol = nullptr;     // [S]
+  RowArgs* d_srow = nullptr;     // [4][S]
+  double args_dt = -1.0;
+  bool ready = false;
+  cudaGraphExec_t graph = nullptr;
+  cudaStream_t cap = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  int64_t launches = 0;
+};
+
+namespace {
+
+template <typename T, int L>
+cudaError_t launch_row_batch_t(const KP* kps, const RowArgs* as, int members, cudaStream_t st) {
+  constexpr int N = 1 << L, RPC = rows_per_cta<T, L>();
+  dim3 grid((N / 2 + 1 + RPC - 1) / RPC, members);
+  k_row_batch<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>
+      <<<grid, RPC * row_group<T, L>(), row_smem<T, L>(), st>>>(kps, as);
+  return cudaGetLastError();
+}
+template <typename T, int L>
+cudaError_t launch_col_batch_t(const KP* kps, const ColArgs* as, int members, cudaStream_t st) {
+  constexpr int N = 1 << L, NP = pairs_per_cta<T, L>();
+  dim3 grid(N / (2 * NP), members);
+  k_col_batch<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()>
+      <<<grid, NP * col_group<T, L>(), col_smem<T, L>(), st>>>(kps, as);
+  return cudaGetLastError();
+}
+template <typename T, int L>
+cudaError_t set_batch_attrs_t() {
+  constexpr int RPC = rows_per_cta<T, L>(), NP = pairs_per_cta<T, L>();
+  cudaError_t e = cudaFuncSetAttribute(k_row_batch<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem<T, L>());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_col_batch<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem<T, L>());
+}
+template <typename T>
+cudaError_t launch_row_batch_p(int log2n, const KP* kps, const RowArgs* as, int m, cudaStream_t st) {
+  SQG_DISPATCH(log2n, launch_row_batch_t, kps, as, m, st);
+}
+template <typename T>
+cudaError_t launch_col_batch_p(int log2n, const KP* kps, const ColArgs* as, int m, cudaStream_t st) {
+  SQG_DISPATCH(log2n, launch_col_batch_t, kps, as, m, st);
+}
+template <typename T>
+cudaError_t set_batch_attrs_p(int log2n) {
+  SQG_DISPATCH(log2n, set_batch_attrs_t);
+}
+
+cudaError_t brow(sqg_batch* b, const KP* kps, const RowArgs* as, int m, cudaStream_t st) {
+  if (m == 0) return cudaSuccess;
+  b->launches++;
+  return b->d.precision == SQG_F64 ? launch_row_batch_p<double>(b->log2N, kps, as, m, st)
+                                   : launch_row_batch_p<float>(b->log2N, kps, as, m, st);
+}
+cudaError_t bcol(sqg_batch* b, const KP* kps, const ColArgs* as, int m, cudaStream_t st) {
+  if (m == 0) return cudaSuccess;
+  b->launches++;
+  return b->d.precision == SQG_F64 ? launch_col_batch_p<double>(b->log2N, kps, as, m, st)
+                                   : launch_col_batch_p<float>(b->log2N, kps, as, m, st);
+}
+
+// Builds and uploads every member's pass arguments for time step dt.
+int batch_upload_args(sqg_batch* b, double dt, cudaStream_t st) {
+  const int M = b->M, S = b->S;
+  sqg_plan* tp = &b->tables;
+  KP base = make_kp(tp, dt);
+  base.ring_on = 0;
+  base.n_ring = 0;
+  std::vector<KP> kp(M), kps(std::max(S, 1));
+  std::vector<RowArgs> p1(M), row(4 * M), sp1(std::max(S, 1)), srow(4 * std::max(S, 1));
+  std::vector<ColArgs> col(M), vel(M), scol(std::max(S, 1));
+  const bool explicit_lin = b->d.scheme == SQG_EXPLICIT_RK4 &&
+                            (b->d.nu_p != 0.0 || (b->d.has_damping && (b->d.mu != 0.0 || b->d.nu_damp != 0.0)));
+  for (int i = 0; i < M; ++i) {
+    unsigned char* mb = b->ws + b->off_member + (size_t)i * b->member_stride;
+    kp[i] = base;
+    kp[i].alpha = b->mem[i].alpha;
+    kp[i].akind = alpha_kind(b->mem[i].alpha);
+    RowArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.fmode = FM_THETA;
+    a.xh = mb + b->m_xh;
+    a.jh = mb + b->m_jh;
+    a.acc = mb + b->m_acc;
+    a.st_out = mb + b->m_stage;
+    a.st_in = a.st_out;
+    a.th_n = b->mem[i].theta;
+    a.th_out = b->mem[i].theta;
+    a.do_p1 = 1;
+    p1[i] = a;
+    p1[i].rmode = RM_P1;
+    for (int s = 1; s <= 4; ++s) {
+      RowArgs r = a;
+      r.rmode = RM_STAGE;
+      r.stage = s;
+      r.stage_write = explicit_lin ? SW_FULL : SW_NONE;
+      row[(s - 1) * M + i] = r;
+    }
+    ColArgs c;
+    std::memset(&c, 0, sizeof(c));
+    c.cmode = CM_THETA;
+    c.xh = a.xh;
+    c.jh = const_cast<void*>(a.jh);
+    col[i] = c;
+    ColArgs v = c;
+    v.cmode = CM_VEL;
+    v.out0 = mb + b->m_uv;
+    v.out1 = nullptr;
+    if (b->mem[i].n_scalars == 0) v.xh = nullptr;  // no work for this member
+    vel[i] = v;
+  }
+  for (int k = 0; k < S; ++k) {
+    const int i = b->scal_member[k], q = b->scal_slot[k];
+    unsigned char* sb = b->ws + b->off_scalar + (size_t)k * b->scalar_stride;
+    unsigned char* mb = b->ws + b->off_member + (size_t)i * b->member_stride;
+    kps[k] = base;
+    RowArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.fmode = FM_SCAL;
+    a.xh = sb + b->s_xs;
+    a.jh = sb + b->s_js;
+    a.acc = sb + b->s_acc;
+    a.st_out = sb + b->s_stage;
+    a.st_in = a.st_out;
+    a.th_n = b->mem[i].scalars[q];
+    a.th_out = b->mem[i].scalars[q];
+    a.kappa = b->mem[i].kappa[q];
+    a.do_p1 = 1;
+    sp1[k] = a;
+    sp1[k].rmode = RM_P1;
+    const bool sexp = b->d.scheme == SQG_EXPLICIT_RK4 && a.kappa != 0.0;
+    for (int s = 1; s <= 4; ++s) {
+      RowArgs r = a;
+      r.rmode = RM_STAGE;
+      r.stage = s;
+      r.do_p1 = s < 4 ? 1 : 0;
+      r.stage_write = sexp ? SW_FULL : SW_NONE;
+      srow[(s - 1) * S + k] = r;
+    }
+    ColArgs c;
+    std::memset(&c, 0, sizeof(c));
+    c.cmode = CM_SCAL;
+    c.xh = a.xh;
+    c.jh = const_cast<void*>(a.jh);
+    c.uv = mb + b->m_uv;
+    scol[k] = c;
+  }
+  auto up = [&](void* dst, const void* src, size_t n) {
+    return cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, st);
+  };
+  SQG_CUDA(up(b->d_kp, kp.data(), M * sizeof(KP)));
+  SQG_CUDA(up(b->d_p1, p1.data(), M * sizeof(RowArgs)));
+  SQG_CUDA(up(b->d_row, row.data(), 4 * M * sizeof(RowArgs)));
+  SQG_CUDA(up(b->d_col, col.data(), M * sizeof(ColArgs)));
+  SQG_CUDA(up(b->d_vel, vel.data(), M * sizeof(ColArgs)));
+  if (S > 0) {
+    SQG_CUDA(up(b->d_kps, kps.data(), S * sizeof(KP)));
+    SQG_CUDA(up(b->d_sp1, sp1.data(), S * sizeof(RowArgs)));
+    SQG_CUDA(up(b->d_srow, srow.data(), 4 * S * sizeof(RowArgs)));
+    SQG_CUDA(up(b->d_scol, scol.data(), S * sizeof(ColArgs)));
+  }
+  SQG_CUDA(cudaStreamSynchronize(st));  // host vectors go out of scope
+  b->args_dt = dt;
+  return SQG_OK;
+}
+
+// One ensemble step after the theta P1 pass of the step's input.
+int batch_step_launches(sqg_batch* b, cudaStream_t st) {
+  const int M = b->M, S = b->S;
+  for (int s = 1; s <= 4; ++s) {
+    SQG_CUDA(bcol(b, b->d_kp, b->d_col, M, st));
+    SQG_CUDA(brow(b, b->d_kp, b->d_row + (size_t)(s - 1) * M, M, st));
+  }
+  if (S > 0) {
+    // u + i v of theta_{n+1} from the stage-4 transforms, then the scalars
+    SQG_CUDA(bcol(b, b->d_kp, b->d_vel, M, st));
+    SQG_CUDA(brow(b, b->d_kps, b->d_sp1, S, st));
+    for (int s = 1; s <= 4; ++s) {
+      SQG_CUDA(bcol(b, b->d_kps, b->d_scol, S, st));
+      SQG_CUDA(brow(b, b->d_kps, b->d_srow + (size_t)(s - 1) * S, S, st));
+    }
+  }
+  return SQG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sqg_batch_create(const sqg_desc* desc, int32_t n_members, const sqg_member* members, sqg_batch** out) {
+  if (!desc || !members || !out || n_members <= 0) return fail(SQG_ERR_INVALID, "bad batch arguments");
+  sqg_desc d = *desc;
+  d.has_ring = 0;
+  d.n_scalars = 0;
+  sqg_plan* tp = nullptr;
+  int rc = sqg_plan_create(&d, &tp);
+  if (rc != SQG_OK) return rc;
+  sqg_batch* b = new sqg_batch();
+  b->tables = *tp;
+  b->tables.off_total = b->tables.off_acc;  // the batch keeps only the grid tables of the plan
+  sqg_plan_destroy(tp);
+  b->d = d;
+  b->N = d.N;
+  b->H = d.N / 2;
+  b->log2N = b->tables.log2N;
+  b->csize = b->tables.csize;
+  b->M = n_members;
+  b->mem.assign(members, members + n_members);
+  for (int i = 0; i < n_members; ++i) {
+    const sqg_member& m = members[i];
+    if (!m.theta) { delete b; return fail(SQG_ERR_INVALID, "member theta is null"); }
+    if (!(m.alpha >= -2 && m.alpha <= 2)) { delete b; return fail(SQG_ERR_INVALID, "alpha must be in [-2, 2]"); }
+    if (m.n_scalars < 0 || m.n_scalars > SQG_MAX_SCALARS) { delete b; return fail(SQG_ERR_INVALID, "n_scalars out of range"); }
+    for (int q = 0; q < m.n_scalars; ++q) {
+      if (!m.scalars[q]) { delete b; return fail(SQG_ERR_INVALID, "member scalar is null"); }
+      b->scal_member.push_back(i);
+      b->scal_slot.push_back(q);
+    }
+  }
+  b->S = (int)b->scal_member.size();
+  const size_t N = b->N, cs = b->csize, full = N * N * cs, half = (N / 2 + 1) * N * cs;
+  auto al = [](size_t x) { return align256(x); };
+  b->m_acc = 0;
+  b->m_stage = al(full);
+  b->m_xh = b->m_stage + al(full);
+  b->m_jh = b->m_xh + al(4 * half);
+  b->m_uv = b->m_jh + al(half);
+  b->member_stride = b->m_uv + al(full);
+  b->s_acc = 0;
+  b->s_stage = al(full);
+  b->s_xs = b->s_stage + al(full);
+  b->s_js = b->s_xs + al(2 * half);
+  b->scalar_stride = b->s_js + al(half);
+  b->off_tab = 0;
+  b->off_member = al(b->tables.off_acc);  // grid tables come first, as in a plan
+  b->off_scalar = b->off_member + (size_t)b->M * b->member_stride;
+  b->off_args = b->off_scalar + (size_t)b->S * b->scalar_stride;
+  const size_t Sx = std::max(b->S, 1);
+  b->off_total = b->off_args + al(b->M * sizeof(KP)) + al(Sx * sizeof(KP)) + al(b->M * sizeof(RowArgs)) +
+                 al(b->M * sizeof(ColArgs)) + al(4 * b->M * sizeof(RowArgs)) + al(b->M * sizeof(ColArgs)) +
+                 al(Sx * sizeof(RowArgs)) + al(Sx * sizeof(ColArgs)) + al(4 * Sx * sizeof(RowArgs));
+  *out = b;
+  return SQG_OK;
+}
+
+int sqg_batch_workspace_bytes(const sqg_batch* b, size_t* bytes) {
+  if (!b || !bytes) return fail(SQG_ERR_INVALID, "null argument");
+  *bytes = b->off_total;
+  return SQG_OK;
+}
+
+int sqg_batch_set_workspace(sqg_batch* b, void* ws, size_t bytes, void* stream) {
+  if (!b) return fail(SQG_ERR_INVALID, "null batch");
+  if (!ws || bytes < b->off_total) return fail(SQG_ERR_WORKSPACE, "workspace missing or too small");
+  cudaStream_t st = (cudaStream_t)stream;
+  // grid tables: the first bytes of the workspace, as a plan lays them out
+  int rc = sqg_plan_set_workspace(&b->tables, ws, b->tables.off_acc, stream);
+  if (rc != SQG_OK) return rc;
+  b->ws = (unsigned char*)ws;
+  b->ws_bytes = bytes;
+  size_t o = b->off_args;
+  auto take = [&](size_t n) { unsigned char* p = b->ws + o; o += align256(n); return p; };
+  const size_t Sx = std::max(b->S, 1);
+  b->d_kp = (KP*)take(b->M * sizeof(KP));
+  b->d_kps = (KP*)take(Sx * sizeof(KP));
+  b->d_p1 = (RowArgs*)take(b->M * sizeof(RowArgs));
+  b->d_col = (ColArgs*)take(b->M * sizeof(ColArgs));
+  b->d_row = (RowArgs*)take(4 * b->M * sizeof(RowArgs));
+  b->d_vel = (ColArgs*)take(b->M * sizeof(ColArgs));
+  b->d_sp1 = (RowArgs*)take(Sx * sizeof(RowArgs));
+  b->d_scol = (ColArgs*)take(Sx * sizeof(ColArgs));
+  b->d_srow = (RowArgs*)take(4 * Sx * sizeof(RowArgs));
+  if (b->d.precision == SQG_F64) { SQG_CUDA(set_batch_attrs_p<double>(b->log2N)); }
+  else { SQG_CUDA(set_batch_attrs_p<float>(b->log2N)); }
+  if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  b->args_dt = -1.0;
+  b->ready = true;
+  (void)st;
+  return SQG_OK;
+}
+
+int sqg_batch_multistep(sqg_batch* b, int32_t n_steps, double dt, int32_t use_graph, void* stream) {
+  if (!b) return fail(SQG_ERR_INVALID, "null batch");
+  if (!b->ready) return fail(SQG_ERR_WORKSPACE, "workspace not set (call sqg_batch_set_workspace)");
+  if (n_steps < 0) return fail(SQG_ERR_INVALID, "n_steps must be >= 0");
+  if (n_steps == 0) return SQG_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  if (b->args_dt != dt) {
+    if ((rc = batch_upload_args(b, dt, st)) != SQG_OK) return rc;
+    if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  }
+  b->launches = 0;
+  // theta P1 of every member's input state
+  SQG_CUDA(brow(b, b->d_kp, b->d_p1, b->M, st));
+  if (!use_graph) {
+    for (int n = 0; n < n_steps; ++n)
+      if ((rc = batch_step_launches(b, st)) != SQG_OK) return rc;
+    return SQG_OK;
+  }
+  if (!b->cap) {
+    SQG_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+    SQG_CUDA(cudaEventCreateWithFlags(&b->ev_in, cudaEventDisableTiming));
+    SQG_CUDA(cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming));
+  }
+  if (!b->graph) {
+    cudaGraph_t g;
+    SQG_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+    const int64_t saved = b->launches;
+    rc = batch_step_launches(b, b->cap);
+    cudaError_t ce = cudaStreamEndCapture(b->cap, &g);
+    const int64_t per_step = b->launches - saved;
+    b->launches = saved;
+    if (rc != SQG_OK) return rc;
+    if (ce != cudaSuccess) return fail(SQG_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) return fail(SQG_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(ce));
+    b->tables.launches = per_step;  // launches in one replay
+  }
+  SQG_CUDA(cudaEventRecord(b->ev_in, st));
+  SQG_CUDA(cudaStreamWaitEvent(b->cap, b->ev_in, 0));
+  for (int n = 0; n < n_steps; ++n) {
+    SQG_CUDA(cudaGraphLaunch(b->graph, b->cap));
+    b->launches += b->tables.launches;
+  }
+  SQG_CUDA(cudaEventRecord(b->ev_out, b->cap));
+  SQG_CUDA(cudaStreamWaitEvent(st, b->ev_out, 0));
+  return SQG_OK;
+}
+
+int sqg_batch_last_launch_count(const sqg_batch* b, int64_t* n) {
+  if (!b || !n) return fail(SQG_ERR_INVALID, "null argument");
+  *n = b->launches;
+  return SQG_OK;
+}
+
+int sqg_batch_destroy(sqg_batch* b) {
+  if (!b) return SQG_OK;
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  if (b->ev_in) cudaEventDestroy(b->ev_in);
+  if (b->ev_out) cudaEventDestroy(b->ev_out);
+  b->tables.graph_exec = nullptr;
+  b->tables.cap_stream = nullptr;
+  b->tables.ev_in = b->tables.ev_out = nullptr;
+  delete b;
+  return SQG_OK;
+}
+
+}  // extern "C"

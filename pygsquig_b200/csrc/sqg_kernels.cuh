@@ -234,8 +234,7 @@ __device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, const
 // cp.async ahead of use; the first DEPTH chunks are requested before the
 // forward FFT of the J row, so their latency hides behind it.
 template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
-__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), min_blocks<T>(RPC * ((1 << LOG2N) / R)))
-k_row(KP kp, RowArgs a) {
+__device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a) {
   using C = typename Cplx<T>::type;
   constexpr int N = 1 << LOG2N;
   constexpr int G = N / R;
@@ -576,8 +575,7 @@ __device__ void ring_reduce(const KP& kp, const ColArgs& a);
 // once (round-2 copies land while round 1 computes); NBUF = 2: two rounds of
 // two fields (large N in float64, where four buffers do not fit).
 template <typename T, int LOG2N, int R, int NP, int NBUF>
-__global__ void __launch_bounds__(NP * ((1 << LOG2N) / R), min_blocks<T>(NP * ((1 << LOG2N) / R)))
-k_col(KP kp, ColArgs a) {
+__device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
   using C = typename Cplx<T>::type;
   constexpr int N = 1 << LOG2N;
   constexpr int G = N / R;
@@ -809,5 +807,40 @@ namespace sqg {
 __global__ void k_set_ctl(RingCtl* ctl, const double* base) {
   ctl->base = base;
   ctl->ctr = 0;
+}
+}  // namespace sqg
+
+namespace sqg {
+// ---- kernels: one plan, or a batch of members (member = blockIdx.y) ----
+template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
+__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), min_blocks<T>(RPC * ((1 << LOG2N) / R)))
+k_row(KP kp, RowArgs a) {
+  row_body<T, LOG2N, R, RPC, DEPTH, NFX>(kp, a);
+}
+
+template <typename T, int LOG2N, int R, int NP, int NBUF>
+__global__ void __launch_bounds__(NP * ((1 << LOG2N) / R), min_blocks<T>(NP * ((1 << LOG2N) / R)))
+k_col(KP kp, ColArgs a) {
+  col_body<T, LOG2N, R, NP, NBUF>(kp, a);
+}
+
+// Batched forms: the member's parameters come from device arrays; members
+// with no work in this pass have a null xh pointer and return at once.
+template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
+__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), min_blocks<T>(RPC * ((1 << LOG2N) / R)))
+k_row_batch(const KP* __restrict__ kps, const RowArgs* __restrict__ as) {
+  const KP kp = kps[blockIdx.y];
+  const RowArgs a = as[blockIdx.y];
+  if (a.xh == nullptr && a.rhs_out == nullptr) return;
+  row_body<T, LOG2N, R, RPC, DEPTH, NFX>(kp, a);
+}
+
+template <typename T, int LOG2N, int R, int NP, int NBUF>
+__global__ void __launch_bounds__(NP * ((1 << LOG2N) / R), min_blocks<T>(NP * ((1 << LOG2N) / R)))
+k_col_batch(const KP* __restrict__ kps, const ColArgs* __restrict__ as) {
+  const KP kp = kps[blockIdx.y];
+  const ColArgs a = as[blockIdx.y];
+  if (a.xh == nullptr) return;
+  col_body<T, LOG2N, R, NP, NBUF>(kp, a);
 }
 }  // namespace sqg
