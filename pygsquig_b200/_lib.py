@@ -102,6 +102,8 @@ SIGNATURES = {
     "sqg_batch_multistep": [_vp, _i32, _dbl, _i32, _vp],
     "sqg_batch_last_launch_count": [_vp, C.POINTER(C.c_int64)],
     "sqg_batch_destroy": [_vp],
+    "closure_conv64": [_i32, _i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp],
+    "closure_last_error_string": [],
     "sqg_last_error_string": [],
     "sqg_version": [],
 }
@@ -125,7 +127,7 @@ def load():
         for name, argt in SIGNATURES.items():
             fn = getattr(lib, name)
             fn.argtypes = argt
-            fn.restype = C.c_char_p if name == "sqg_last_error_string" else C.c_int
+            fn.restype = C.c_char_p if name.endswith("_last_error_string") else C.c_int
         _lib = lib
         return lib
 

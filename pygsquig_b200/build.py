@@ -11,9 +11,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = os.path.join(HERE, "csrc", "sqg_capi.cu")
+SRCS = [os.path.join(HERE, "csrc", f) for f in ("sqg_capi.cu", "closure_conv.cu")]
 DEPS = [os.path.join(HERE, "csrc", f) for f in ("sqg_fft.cuh", "sqg_kernels.cuh", "sqg_aux.cuh")] + [
-    os.path.join(ROOT, "include", "sqg.h")]
+    os.path.join(ROOT, "include", f) for f in ("sqg.h", "sqg_closure.h")]
 OUT = os.path.join(HERE, "libsqg.so")
 
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
@@ -31,13 +31,13 @@ def up_to_date() -> bool:
     if not os.path.exists(OUT):
         return False
     t = os.path.getmtime(OUT)
-    return all(os.path.getmtime(p) <= t for p in [SRC] + DEPS)
+    return all(os.path.getmtime(p) <= t for p in SRCS + DEPS)
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return OUT
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", OUT + ".tmp", SRC]
+    cmd = [nvcc()] + NVCC_FLAGS + ["-o", OUT + ".tmp"] + SRCS
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -1,0 +1,405 @@
+// closure_conv.cu -- BF16 tensor-core (tcgen05) 3x3 convolution with 64 input
+// and 64 output channels for the learned subgrid closure.
+//
+// Implicit GEMM: M = 128 pixels of one image row (a tile), N = 64 output
+// channels, K = 9 taps x 64 input channels (one 64-wide K block per tap).
+// Activations are NHWC BF16 with a one-pixel circular halo, so the A block of
+// tap (dy, dx) is 128 consecutive pixel rows of 128 bytes: one TMA box
+// (128B-swizzled) straight from the halo'd tensor.  The weights of the 9 taps
+// stay in shared memory for the life of the persistent CTA.
+//
+// Warp roles (6 warps): warp 0 issues TMA loads, warp 1 allocates TMEM and
+// issues the MMAs (one elected thread), warps 2..5 read the FP32 accumulators
+// from TMEM (tcgen05.ld, one lane quarter each) and run the epilogue.  Two
+// TMEM accumulators alternate so the epilogue of tile i overlaps the MMAs of
+// tile i+1.  Every mbarrier wait is bounded: on time-out the kernel records
+// an error flag and the roles drain and return.
+//
+// Epilogues:
+//   FWD:   z = acc + bias; store z (BF16, unpadded) and gelu(z) (BF16, halo'd)
+//   DGRAD: g = acc * gelu'(zprev); store g (BF16, halo'd)
+//   LIN:   store acc + bias (FP32, unpadded)
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstring>
+#include <string>
+
+#include "../../include/sqg_closure.h"
+
+namespace {
+
+thread_local std::string g_err;
+int cfail(int code, const std::string& m) {
+  g_err = m;
+  return code;
+}
+
+constexpr int kStages = 6;
+constexpr int kTileM = 128;
+constexpr int kC = 64;
+constexpr int kABytes = kTileM * kC * 2;  // 16 KB per tap slice
+constexpr int kBBytes = kC * kC * 2;      // 8 KB per tap
+constexpr int kThreads = 192;
+constexpr uint32_t kWaitLimit = 1u << 26;
+
+// ---- PTX helpers ------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes));
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)));
+}
+// Bounded wait on the phase parity; returns false on time-out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+__device__ __forceinline__ uint64_t sw128_desc(const void* smem_tile) {
+  // K-major, 128-byte swizzle: rows of 128 B, 8-row groups 1024 B apart
+  const uint64_t start = (smem_u32(smem_tile) >> 4) & 0x3FFF;
+  const uint64_t lbo = 1, sbo = 1024 >> 4;
+  return start | (lbo << 16) | (sbo << 32) | (1ull << 46) | (2ull << 61);
+}
+// BF16 x BF16 -> FP32, K-major A and B, M = 128, N = 64
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+#define TC_LD32(addr, r)                                                                                      \
+  asm volatile(                                                                                               \
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"      \
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"                            \
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),     \
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), \
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),           \
+        "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),           \
+        "=r"(r[30]), "=r"(r[31])                                                                              \
+      : "r"(addr))
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float z) {
+  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+}
+
+struct ConvArgs {
+  int B, H, W;            // images, rows, columns (W multiple of 128)
+  int mode;               // CLOSURE_EPI_*
+  const float* bias;      // [64] (FWD, LIN)
+  const __nv_bfloat16* zprev;  // [B][H][W][64] pre-activation of the layer below (DGRAD)
+  __nv_bfloat16* out_pad;      // [B][H+2][W+2][64] halo'd output (FWD: gelu(z), DGRAD: g)
+  __nv_bfloat16* out_z;        // [B][H][W][64] pre-activation (FWD)
+  float* out_f32;              // [B][H][W][64] (LIN)
+  unsigned* err;
+};
+
+// Writes the 64 BF16 values of pixel (b, y, x) to the halo'd tensor,
+// including its circular copies on the halo.
+__device__ __forceinline__ void store_halo(__nv_bfloat16* out, int H, int W, int b, int y, int x,
+                                           const uint4 (&v)[8]) {
+  const int Wp = W + 2, Hp = H + 2;
+  int ys[2] = {y + 1, -1}, xs[2] = {x + 1, -1};
+  if (y == 0) ys[1] = H + 1;
+  if (y == H - 1) ys[1] = 0;
+  if (x == 0) xs[1] = W + 1;
+  if (x == W - 1) xs[1] = 0;
+  for (int a = 0; a < 2; ++a) {
+    if (ys[a] < 0) continue;
+    for (int c = 0; c < 2; ++c) {
+      if (xs[c] < 0) continue;
+      uint4* dst = reinterpret_cast<uint4*>(out + (((size_t)b * Hp + ys[a]) * Wp + xs[c]) * kC);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) dst[i] = v[i];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CUtensorMap w_map, ConvArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 1024-byte aligned carve-up
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char* sB = base;                          // 9 x 8 KB weights
+  unsigned char* sA = base + 9 * kBBytes;            // kStages x 16 KB activations
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sA + kStages * kABytes);
+  uint64_t* full = bars;                 // [kStages]
+  uint64_t* empty = bars + kStages;      // [kStages]
+  uint64_t* acc_full = bars + 2 * kStages;   // [2]
+  uint64_t* acc_empty = acc_full + 2;        // [2]
+  uint64_t* wbar = acc_empty + 2;            // [1] weights; wbar[2] drain
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(wbar + 3);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tiles_per_row = a.W / kTileM;
+  const int n_tiles = a.B * a.H * tiles_per_row;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&acc_full[i], 1);
+      mbar_init(&acc_empty[i], 4);  // one arrive per epilogue warp
+    }
+    mbar_init(wbar, 1);
+    mbar_init(wbar + 2, 1);  // drain barrier of the error path
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                 "r"(128));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  bool ok = true;
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      mbar_expect_tx(wbar, 9 * kBBytes);
+      for (int t = 0; t < 9; ++t) tma_load_2d(sB + t * kBBytes, &w_map, wbar, 0, t * kC);
+      int it = 0;
+      for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+        const int xt = tile % tiles_per_row;
+        const int rowi = tile / tiles_per_row;
+        const int y = rowi % a.H, b = rowi / a.H;
+        for (int t = 0; t < 9 && ok; ++t, ++it) {
+          const int s = it % kStages;
+          const uint32_t ph = (it / kStages) & 1;
+          if (it >= kStages && !mbar_wait(&empty[s], ph ^ 1)) { ok = false; break; }
+          const int dy = t / 3 - 1, dx = t % 3 - 1;
+          const int q = (b * (a.H + 2) + (y + 1 + dy)) * (a.W + 2) + (xt * kTileM + 1 + dx);
+          mbar_expect_tx(&full[s], kABytes);
+          tma_load_2d(sA + s * kABytes, &act_map, &full[s], 0, q);
+        }
+      }
+      if (!ok) {
+        atomicOr(a.err, 1u);
+        // drain: wait (bounded) for the copies still in flight
+        for (int i = (it > kStages ? it - kStages : 0); i < it; ++i) mbar_wait(&full[i % kStages], (i / kStages) & 1);
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      ok = mbar_wait(wbar, 0);
+      int it = 0, tcount = 0;
+      for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x, ++tcount) {
+        const int acc = tcount & 1;
+        const uint32_t aph = (tcount >> 1) & 1;
+        if (tcount >= 2 && !mbar_wait(&acc_empty[acc], aph ^ 1)) { ok = false; break; }
+        tc_fence_after();
+        const uint32_t d = tmem + acc * 64;
+        for (int t = 0; t < 9 && ok; ++t, ++it) {
+          const int s = it % kStages;
+          const uint32_t ph = (it / kStages) & 1;
+          if (!mbar_wait(&full[s], ph)) { ok = false; break; }
+          tc_fence_after();
+          const uint64_t ad = sw128_desc(sA + s * kABytes);
+          const uint64_t bd = sw128_desc(sB + t * kBBytes);
+#pragma unroll
+          for (int k = 0; k < 4; ++k)  // K = 16 per MMA: 32 bytes along the 128-byte row
+            umma(d, ad + 2 * k, bd + 2 * k, (t > 0 || k > 0) ? 1u : 0u);
+          umma_commit(&empty[s]);  // frees the slot when these MMAs complete
+        }
+        umma_commit(&acc_full[acc]);
+      }
+      if (!ok) {
+        atomicOr(a.err, 2u);
+        // drain: wait (bounded) until every MMA issued so far has completed
+        umma_commit(wbar + 2);
+        mbar_wait(wbar + 2, 0);
+      }
+    }
+  } else {
+    // ---------------- epilogue (warps 2..5) ----------------
+    const int quarter = warp & 3;  // TMEM lane quarter this warp may access
+    const int row = quarter * 32 + lane;
+    int tcount = 0;
+    for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x, ++tcount) {
+      const int acc = tcount & 1;
+      const uint32_t aph = (tcount >> 1) & 1;
+      if (!mbar_wait(&acc_full[acc], aph)) { ok = false; break; }
+      tc_fence_after();
+      float v[64];
+      uint32_t r[32];
+      const uint32_t taddr = tmem + acc * 64 + ((uint32_t)(quarter * 32) << 16);
+      TC_LD32(taddr, r);
+#pragma unroll
+      for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+      TC_LD32(taddr + 32, r);
+#pragma unroll
+      for (int i = 0; i < 32; ++i) v[32 + i] = __uint_as_float(r[i]);
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[acc]);
+      // pixel of this thread
+      const int xt = tile % tiles_per_row;
+      const int rowi = tile / tiles_per_row;
+      const int y = rowi % a.H, b = rowi / a.H;
+      const int x = xt * kTileM + row;
+      const size_t pix = ((size_t)b * a.H + y) * a.W + x;
+      if (a.mode == CLOSURE_EPI_LIN) {
+        float4* o = reinterpret_cast<float4*>(a.out_f32 + pix * kC);
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          o[i] = make_float4(v[4 * i] + a.bias[4 * i], v[4 * i + 1] + a.bias[4 * i + 1],
+                             v[4 * i + 2] + a.bias[4 * i + 2], v[4 * i + 3] + a.bias[4 * i + 3]);
+        continue;
+      }
+      uint4 packed[8];
+      if (a.mode == CLOSURE_EPI_FWD) {
+        uint4 zp[8];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          const float z0 = v[2 * i] + a.bias[2 * i], z1 = v[2 * i + 1] + a.bias[2 * i + 1];
+          const __nv_bfloat162 zb = __floats2bfloat162_rn(z0, z1);
+          const float2 zr = __bfloat1622float2(zb);  // the stored pre-activation
+          const __nv_bfloat162 g = __floats2bfloat162_rn(gelu(zr.x), gelu(zr.y));
+          reinterpret_cast<__nv_bfloat162*>(zp)[i] = zb;
+          reinterpret_cast<__nv_bfloat162*>(packed)[i] = g;
+        }
+        uint4* oz = reinterpret_cast<uint4*>(a.out_z + pix * kC);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) oz[i] = zp[i];
+      } else {  // DGRAD
+        const uint4* zsrc = reinterpret_cast<const uint4*>(a.zprev + pix * kC);
+        uint4 zq[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) zq[i] = zsrc[i];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          const float2 z = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(zq)[i]);
+          reinterpret_cast<__nv_bfloat162*>(packed)[i] =
+              __floats2bfloat162_rn(v[2 * i] * gelu_grad(z.x), v[2 * i + 1] * gelu_grad(z.y));
+        }
+      }
+      store_halo(a.out_pad, a.H, a.W, b, y, x, packed);
+    }
+    if (!ok) atomicOr(a.err, 4u);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(128));
+  }
+}
+
+// ---- host: tensor maps through the driver entry point -------------------------
+typedef CUresult (*PFN_encodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+PFN_encodeTiled encode_fn() {
+  static PFN_encodeTiled fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_encodeTiled)p;
+  }
+  return fn;
+}
+
+// rows x 64 BF16 matrix, row stride 128 B, boxes of box_rows x 64, 128B swizzle
+bool make_map(CUtensorMap* m, const void* ptr, uint64_t rows, uint32_t box_rows) {
+  PFN_encodeTiled f = encode_fn();
+  if (!f) return false;
+  cuuint64_t dims[2] = {kC, rows};
+  cuuint64_t strides[1] = {kC * 2};
+  cuuint32_t box[2] = {kC, box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
+           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+constexpr size_t kSmemBytes = 1024 + 9 * kBBytes + kStages * kABytes + 256;
+
+}  // namespace
+
+extern "C" {
+
+const char* closure_last_error_string(void) { return g_err.c_str(); }
+
+int closure_conv64(int32_t B, int32_t H, int32_t W, int32_t mode, const void* act_pad, const void* weights,
+                   const float* bias, const void* zprev, void* out_pad, void* out_z, float* out_f32,
+                   uint32_t* err, int32_t grid, void* stream) {
+  if (B <= 0 || H <= 0 || W <= 0 || W % kTileM != 0)
+    return cfail(1, "closure_conv64: W must be a positive multiple of 128");
+  if (!act_pad || !weights || !err) return cfail(1, "closure_conv64: null pointer");
+  if ((uintptr_t)act_pad % 16 || (uintptr_t)weights % 16) return cfail(1, "closure_conv64: pointers must be 16-byte aligned");
+  if (mode == CLOSURE_EPI_FWD && (!bias || !out_pad || !out_z)) return cfail(1, "closure_conv64: FWD needs bias, out_pad, out_z");
+  if (mode == CLOSURE_EPI_DGRAD && (!zprev || !out_pad)) return cfail(1, "closure_conv64: DGRAD needs zprev, out_pad");
+  if (mode == CLOSURE_EPI_LIN && (!bias || !out_f32)) return cfail(1, "closure_conv64: LIN needs bias, out_f32");
+  CUtensorMap amap, wmap;
+  const uint64_t prows = (uint64_t)B * (H + 2) * (W + 2);
+  if (!make_map(&amap, act_pad, prows, kTileM) || !make_map(&wmap, weights, 9 * kC, kC))
+    return cfail(2, "closure_conv64: tensor map encoding failed");
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_conv64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes) != cudaSuccess)
+      return cfail(2, "closure_conv64: shared memory attribute");
+    attr = true;
+  }
+  ConvArgs a;
+  a.B = B; a.H = H; a.W = W; a.mode = mode; a.bias = bias;
+  a.zprev = (const __nv_bfloat16*)zprev;
+  a.out_pad = (__nv_bfloat16*)out_pad;
+  a.out_z = (__nv_bfloat16*)out_z;
+  a.out_f32 = out_f32;
+  a.err = err;
+  const int n_tiles = B * H * (W / kTileM);
+  int g = grid > 0 ? grid : 148;
+  if (g > n_tiles) g = n_tiles;
+  k_conv64<<<g, kThreads, kSmemBytes, (cudaStream_t)stream>>>(amap, wmap, a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cfail(2, std::string("closure_conv64 launch: ") + cudaGetErrorString(e));
+  return 0;
+}
+
+}  // extern "C"
