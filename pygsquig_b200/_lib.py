@@ -103,6 +103,15 @@ SIGNATURES = {
     "sqg_batch_last_launch_count": [_vp, C.POINTER(C.c_int64)],
     "sqg_batch_destroy": [_vp],
     "closure_conv64": [_i32, _i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp],
+    "closure_wgrad64": [_i32, _i32, _i32, _vp, _vp, _vp, _i32, _vp, _vp, _vp],
+    "closure_conv_in": [_i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp],
+    "closure_conv_out": [_i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp],
+    "closure_conv_out_dgrad": [_i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp],
+    "closure_small_grad": [_i32, _i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "closure_mse": [C.c_int64, _vp, _vp, _vp, _vp, _vp],
+    "closure_adam": [C.c_int64, _vp, _vp, _vp, _vp, C.c_float, C.c_float, C.c_float, C.c_float, _i32, _vp],
+    "closure_weights_bf16": [_vp, _vp, _vp, _vp],
+    "closure_ops_last_error_string": [],
     "closure_last_error_string": [],
     "sqg_last_error_string": [],
     "sqg_version": [],

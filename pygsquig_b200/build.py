@@ -11,7 +11,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRCS = [os.path.join(HERE, "csrc", f) for f in ("sqg_capi.cu", "closure_conv.cu")]
+SRCS = [os.path.join(HERE, "csrc", f) for f in ("sqg_capi.cu", "closure_conv.cu", "closure_ops.cu")]
 DEPS = [os.path.join(HERE, "csrc", f) for f in ("sqg_fft.cuh", "sqg_kernels.cuh", "sqg_aux.cuh")] + [
     os.path.join(ROOT, "include", f) for f in ("sqg.h", "sqg_closure.h")]
 OUT = os.path.join(HERE, "libsqg.so")

@@ -34,3 +34,17 @@ def conv64(act_pad: torch.Tensor, weights: torch.Tensor, mode: int, bias=None, z
     check(lib().closure_conv64(B, Hp - 2, Wp - 2, mode, _p(act_pad), _p(weights), _p(bias), _p(zprev), _p(out_pad),
                                _p(out_z), _p(out_f32), _p(err), grid, torch.cuda.current_stream().cuda_stream))
     return err
+
+
+def wgrad64(act_pad: torch.Tensor, grad_pad: torch.Tensor, nparts: int = 148, err=None, partials=None):
+    """dW[t, co, ci] = sum_p act[p + off_t, ci] grad[p, co] (FP32 [9, 64, 64])."""
+    B, Hp, Wp, Cc = act_pad.shape
+    assert grad_pad.shape == act_pad.shape and Cc == 64
+    if err is None:
+        err = torch.zeros(1, dtype=torch.int32, device=act_pad.device)
+    if partials is None:
+        partials = torch.empty(nparts * 5 * 128 * 64, dtype=torch.float32, device=act_pad.device)
+    dw = torch.empty(9, 64, 64, dtype=torch.float32, device=act_pad.device)
+    check(lib().closure_wgrad64(B, Hp - 2, Wp - 2, _p(act_pad), _p(grad_pad), _p(partials), nparts, _p(dw), _p(err),
+                                torch.cuda.current_stream().cuda_stream))
+    return dw, err

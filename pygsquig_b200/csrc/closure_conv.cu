@@ -328,6 +328,169 @@ k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CU
   }
 }
 
+// ---- weight gradient: D[(tap, ci)][co] = sum_p a[p + off_tap][ci] g[p][co] ----
+// M = 128 rows = two taps x 64 input channels (MN-major A: the channel index
+// is contiguous in the NHWC rows), N = 64 output channels (MN-major B),
+// K = pixels in blocks of 64 of one image row.  Five accumulators (taps
+// (0,1) (2,3) (4,5) (6,7) (8,-)) live in TMEM; each persistent CTA sums a
+// range of pixel blocks and writes its partial sums; k_wgrad_reduce adds the
+// partials in a fixed order.
+constexpr int kWStages = 2;
+constexpr int kWSlot = 64 * kC * 2;             // 8 KB: 64 pixel rows x 64 channels
+constexpr int kWStageBytes = 11 * kWSlot;       // 10 activation slots + 1 gradient slot
+// MN-major A/B, BF16 -> FP32, M = 128, N = 64
+constexpr uint32_t kIdescMN =
+    (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ uint64_t sw128_mn_desc(const void* smem_tile, uint32_t lbo_bytes) {
+  // MN-major, 128-byte swizzle: 64 elements (128 B) contiguous along M/N,
+  // 8 K-rows per 1024 B atom (SBO); the next 64 M/N elements lbo_bytes away
+  const uint64_t start = (smem_u32(smem_tile) >> 4) & 0x3FFF;
+  const uint64_t lbo = (lbo_bytes >> 4) & 0x3FFF, sbo = 1024 >> 4;
+  return start | (lbo << 16) | (sbo << 32) | (1ull << 46) | (2ull << 61);
+}
+__device__ __forceinline__ void umma_mn(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kIdescMN), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+struct WgradArgs {
+  int B, H, W;
+  float* partials;  // [gridDim.x][5][128][64]
+  unsigned* err;
+};
+
+__global__ void __launch_bounds__(kThreads, 1)
+k_wgrad64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CUtensorMap g_map, WgradArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kWStages * kWStageBytes);
+  uint64_t* full = bars;                 // [kWStages]
+  uint64_t* empty = bars + kWStages;     // [kWStages]
+  uint64_t* acc_full = bars + 2 * kWStages;
+  uint64_t* drain = acc_full + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int bpr = a.W / 64;  // pixel blocks per image row
+  const int n_kb = a.B * a.H * bpr;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kWStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(acc_full, 1);
+    mbar_init(drain, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  bool ok = true;
+  if (warp == 0) {
+    if (lane == 0) {
+      int it = 0;
+      for (int kb = blockIdx.x; kb < n_kb && ok; kb += gridDim.x, ++it) {
+        const int s = it % kWStages;
+        const uint32_t ph = (it / kWStages) & 1;
+        if (it >= kWStages && !mbar_wait(&empty[s], ph ^ 1)) { ok = false; break; }
+        const int xb = kb % bpr, rowi = kb / bpr;
+        const int y = rowi % a.H, b = rowi / a.H;
+        unsigned char* st = base + s * kWStageBytes;
+        mbar_expect_tx(&full[s], 10 * kWSlot);
+        for (int t = 0; t < 9; ++t) {
+          const int dy = t / 3 - 1, dx = t % 3 - 1;
+          const int q = (b * (a.H + 2) + (y + 1 + dy)) * (a.W + 2) + (xb * 64 + 1 + dx);
+          tma_load_2d(st + t * kWSlot, &act_map, &full[s], 0, q);
+        }
+        const int qg = (b * (a.H + 2) + (y + 1)) * (a.W + 2) + (xb * 64 + 1);
+        tma_load_2d(st + 10 * kWSlot, &g_map, &full[s], 0, qg);
+      }
+      if (!ok) {
+        atomicOr(a.err, 8u);
+        for (int i = (it > kWStages ? it - kWStages : 0); i < it; ++i) mbar_wait(&full[i % kWStages], (i / kWStages) & 1);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      int it = 0;
+      for (int kb = blockIdx.x; kb < n_kb && ok; kb += gridDim.x, ++it) {
+        const int s = it % kWStages;
+        const uint32_t ph = (it / kWStages) & 1;
+        if (!mbar_wait(&full[s], ph)) { ok = false; break; }
+        tc_fence_after();
+        unsigned char* st = base + s * kWStageBytes;
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {  // K = 16 pixel rows = two 1024 B atoms
+            const uint64_t ad = sw128_mn_desc(st + (2 * m) * kWSlot, kWSlot) + 128 * k;
+            const uint64_t bd = sw128_mn_desc(st + 10 * kWSlot, kWSlot) + 128 * k;
+            umma_mn(tmem + m * 64, ad, bd, (it > 0 || k > 0) ? 1u : 0u);
+          }
+        }
+        umma_commit(&empty[s]);
+      }
+      umma_commit(acc_full);
+      if (!ok) atomicOr(a.err, 16u);
+    }
+  } else {
+    const int quarter = warp & 3;
+    const int row = quarter * 32 + lane;  // (tap parity, ci)
+    if (blockIdx.x < n_kb) {
+      if (!mbar_wait(acc_full, 0)) ok = false;
+    }
+    tc_fence_after();
+    float* part = a.partials + (size_t)blockIdx.x * 5 * 128 * 64;
+    for (int m = 0; m < 5; ++m) {
+      uint32_t r[32];
+      float v[64];
+      const uint32_t taddr = tmem + m * 64 + ((uint32_t)(quarter * 32) << 16);
+      if (ok && blockIdx.x < n_kb) {
+        TC_LD32(taddr, r);
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+        TC_LD32(taddr + 32, r);
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[32 + i] = __uint_as_float(r[i]);
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      } else {
+#pragma unroll
+        for (int i = 0; i < 64; ++i) v[i] = 0.f;
+      }
+      float4* o = reinterpret_cast<float4*>(part + ((size_t)m * 128 + row) * 64);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+    }
+    if (!ok) atomicOr(a.err, 32u);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(512));
+  }
+}
+
+// dW[t][co][ci] = sum over CTAs of partials[cta][t/2][(t%2)*64 + ci][co]
+__global__ void k_wgrad_reduce(const float* __restrict__ partials, int nparts, float* __restrict__ dw) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;  // over 9 * 64 * 64
+  if (idx >= 9 * 64 * 64) return;
+  const int t = idx / 4096, co = (idx / 64) % 64, ci = idx % 64;
+  const size_t off = ((size_t)(t / 2) * 128 + (t % 2) * 64 + ci) * 64 + co;
+  float s = 0.f;
+  for (int c = 0; c < nparts; ++c) s += partials[(size_t)c * 5 * 128 * 64 + off];
+  dw[idx] = s;
+}
+
 // ---- host: tensor maps through the driver entry point -------------------------
 typedef CUresult (*PFN_encodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                     const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -399,6 +562,31 @@ int closure_conv64(int32_t B, int32_t H, int32_t W, int32_t mode, const void* ac
   k_conv64<<<g, kThreads, kSmemBytes, (cudaStream_t)stream>>>(amap, wmap, a);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cfail(2, std::string("closure_conv64 launch: ") + cudaGetErrorString(e));
+  return 0;
+}
+
+int closure_wgrad64(int32_t B, int32_t H, int32_t W, const void* act_pad, const void* grad_pad, float* partials,
+                    int32_t nparts, float* dw, uint32_t* err, void* stream) {
+  if (B <= 0 || H <= 0 || W <= 0 || W % 64 != 0) return cfail(1, "closure_wgrad64: W must be a positive multiple of 64");
+  if (!act_pad || !grad_pad || !partials || !dw || !err || nparts <= 0) return cfail(1, "closure_wgrad64: bad arguments");
+  CUtensorMap amap, gmap;
+  const uint64_t prows = (uint64_t)B * (H + 2) * (W + 2);
+  if (!make_map(&amap, act_pad, prows, 64) || !make_map(&gmap, grad_pad, prows, 64))
+    return cfail(2, "closure_wgrad64: tensor map encoding failed");
+  static bool attr = false;
+  const size_t smem = 1024 + kWStages * kWStageBytes + 128;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_wgrad64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return cfail(2, "closure_wgrad64: shared memory attribute");
+    attr = true;
+  }
+  WgradArgs a;
+  a.B = B; a.H = H; a.W = W; a.partials = partials; a.err = err;
+  cudaStream_t st = (cudaStream_t)stream;
+  k_wgrad64<<<nparts, kThreads, smem, st>>>(amap, gmap, a);
+  k_wgrad_reduce<<<(9 * 4096 + 255) / 256, 256, 0, st>>>(partials, nparts, dw);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cfail(2, std::string("closure_wgrad64 launch: ") + cudaGetErrorString(e));
   return 0;
 }
 

@@ -60,3 +60,28 @@ def test_conv64_forward_and_dgrad(B, H, W):
     gprime = 0.5 * (1 + torch.erf(zf / 2**0.5)) + zf * torch.exp(-0.5 * zf * zf) / (2 * torch.pi) ** 0.5
     gr = (ref_conv(x.float(), w.float(), None) * gprime).to(torch.bfloat16)
     assert torch.allclose(go.float(), halo(gr).float(), atol=2e-2 * gr.float().abs().max().item(), rtol=2e-2)
+
+
+@pytest.mark.parametrize("B,H,W", [(1, 4, 128), (2, 8, 256)])
+def test_wgrad64(B, H, W):
+    from pygsquig_b200.build import build
+
+    build()
+    from pygsquig_b200.closure import _ops
+
+    torch.manual_seed(1)
+    dev = "cuda"
+    a = torch.randn(B, H, W, 64, device=dev).to(torch.bfloat16)
+    g = torch.randn(B, H, W, 64, device=dev).to(torch.bfloat16)
+    dw, err = _ops.wgrad64(halo(a), halo(g), nparts=7)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    # reference: dW[t, co, ci] = sum_p a[p + off_t, ci] g[p, co]
+    ap = halo(a).float()
+    ref = torch.empty(9, 64, 64, device=dev)
+    for t in range(9):
+        dy, dx = t // 3 - 1, t % 3 - 1
+        sh = ap[:, 1 + dy:1 + dy + H, 1 + dx:1 + dx + W, :]
+        ref[t] = torch.einsum("bhwo,bhwi->oi", g.float(), sh)
+    e = (dw - ref).abs().max().item() / ref.abs().max().item()
+    assert e < 1e-4, e
