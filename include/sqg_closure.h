@@ -43,10 +43,14 @@ int closure_conv64(int32_t B, int32_t H, int32_t W, int32_t mode, const void* ac
 int closure_wgrad64(int32_t B, int32_t H, int32_t W, const void* act_pad, const void* grad_pad, float* partials,
                     int32_t nparts, float* dw, uint32_t* err, void* stream);
 
-/* CUDA-core kernels of the 1-channel layers and the training step.
- * conv_in:  z = conv3x3(x; w[9][64]) + bias (1 -> 64); z BF16 [B][H][W][64],
- *           a_pad = gelu(z) BF16 halo'd.  x: FP32 [B][H][W].
- * conv_out: y = conv3x3(a; w[9][64]) + bias[0] (64 -> 1), y FP32 [B][H][W].
+/* CUDA-core kernels of the 1-channel layers and the training step
+ * (W a multiple of 32, H >= 2; a warp owns 32 pixels of a row, a lane a
+ * channel pair).
+ * conv_in:  z = conv3x3(in_scale x; w[9][64]) + bias (1 -> 64); z BF16
+ *           [B][H][W][64], a_pad = gelu(z) BF16 halo'd.  x: FP32 [B][H][W].
+ * conv_out: y = out_scale (conv3x3(a; w[9][64]) + bias[0]) (64 -> 1), y FP32
+ *           [B][H][W].  (The scales fold an input / output normalisation
+ *           into the layers; training passes 1.)
  * conv_out_dgrad: gz_pad = (sum_t gy[q - off_t] w[t][c]) * gelu'(z[q][c]).
  * small_grad: mode 0 -> out[t*64+c] = sum_p gy[p] a[p+off_t][c], out[576] = sum gy;
  *             mode 1 -> out[t*64+c] = sum_p gz[p][c] x[p+off_t], out[576+c] = sum_p gz[p][c];
@@ -54,10 +58,10 @@ int closure_wgrad64(int32_t B, int32_t H, int32_t W, const void* act_pad, const 
  * mse: gy = 2 (y - t) / n; partials[296] = per-block sums of (y - t)^2.
  * adam: bias-corrected Adam step number `step` (>= 1) on a flat FP32 vector.
  * weights_bf16: wf[t][co][ci] = w, wb[8-t][ci][co] = w (backward-data form). */
-int closure_conv_in(int32_t B, int32_t H, int32_t W, const float* x, const float* w, const float* bias, void* z,
-                    void* a_pad, void* stream);
-int closure_conv_out(int32_t B, int32_t H, int32_t W, const void* a_pad, const float* w, const float* bias, float* y,
-                     void* stream);
+int closure_conv_in(int32_t B, int32_t H, int32_t W, float in_scale, const float* x, const float* w, const float* bias,
+                    void* z, void* a_pad, void* stream);
+int closure_conv_out(int32_t B, int32_t H, int32_t W, float out_scale, const void* a_pad, const float* w,
+                     const float* bias, float* y, void* stream);
 int closure_conv_out_dgrad(int32_t B, int32_t H, int32_t W, const float* gy, const float* w, const void* z,
                            void* gz_pad, void* stream);
 int closure_small_grad(int32_t mode, int32_t B, int32_t H, int32_t W, const float* gy, const void* a_pad,

@@ -104,8 +104,8 @@ SIGNATURES = {
     "sqg_batch_destroy": [_vp],
     "closure_conv64": [_i32, _i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp],
     "closure_wgrad64": [_i32, _i32, _i32, _vp, _vp, _vp, _i32, _vp, _vp, _vp],
-    "closure_conv_in": [_i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp],
-    "closure_conv_out": [_i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp],
+    "closure_conv_in": [_i32, _i32, _i32, C.c_float, _vp, _vp, _vp, _vp, _vp, _vp],
+    "closure_conv_out": [_i32, _i32, _i32, C.c_float, _vp, _vp, _vp, _vp, _vp],
     "closure_conv_out_dgrad": [_i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp],
     "closure_small_grad": [_i32, _i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "closure_mse": [C.c_int64, _vp, _vp, _vp, _vp, _vp],

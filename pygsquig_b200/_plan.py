@@ -164,8 +164,9 @@ class Plan:
         return t.contiguous()
 
     # ---- calls ----
-    def rhs(self, th):
-        out = torch.empty_like(th)
+    def rhs(self, th, out=None):
+        if out is None:
+            out = torch.empty_like(th)
         _lib.check(self._lib.sqg_rhs(self._h, th.data_ptr(), out.data_ptr(), _stream_ptr()))
         return out
 
@@ -192,15 +193,17 @@ class Plan:
         _lib.check(self._lib.sqg_velocity(self._h, th.data_ptr(), u.data_ptr(), v.data_ptr(), _stream_ptr()))
         return u, v
 
-    def to_physical(self, fh):
+    def to_physical(self, fh, out=None):
         N = self.key.N
-        out = torch.empty((N, N), dtype=self.rdtype, device=self.device)
+        if out is None:
+            out = torch.empty((N, N), dtype=self.rdtype, device=self.device)
         _lib.check(self._lib.sqg_to_physical(self._h, fh.data_ptr(), out.data_ptr(), _stream_ptr()))
         return out
 
-    def to_spectral(self, f):
+    def to_spectral(self, f, out=None):
         N = self.key.N
-        out = torch.empty((N, N), dtype=self.cdtype, device=self.device)
+        if out is None:
+            out = torch.empty((N, N), dtype=self.cdtype, device=self.device)
         _lib.check(self._lib.sqg_to_spectral(self._h, f.data_ptr(), out.data_ptr(), _stream_ptr()))
         return out
 

@@ -81,8 +81,11 @@ class ClosureCNN:
             _chk(L.closure_weights_bf16(self.p[f"w{l}"].data_ptr(), self.wf[l].data_ptr(), self.wb[l].data_ptr(), _sp()))
 
     # ---- forward / backward ----
-    def forward(self, x: torch.Tensor) -> torch.Tensor:
-        """x: FP32 [B, H, W] -> y: FP32 [B, H, W] (a view of an internal buffer)."""
+    def forward(self, x: torch.Tensor, in_scale: float = 1.0, out_scale: float = 1.0) -> torch.Tensor:
+        """x: FP32 [B, H, W] -> y: FP32 [B, H, W] (a view of an internal buffer).
+
+        ``in_scale`` / ``out_scale`` multiply the input and the output (a data
+        normalisation folded into the first and last layers)."""
         L = _lib.load()
         B = x.shape[0]
         assert x.shape[1:] == (self.H, self.W) and B <= self.maxB and x.dtype == torch.float32
@@ -90,13 +93,13 @@ class ClosureCNN:
         H, W = self.H, self.W
         a = {l: self.a[l][:B] for l in self.a}
         z = {l: self.z[l][:B] for l in self.z}
-        _chk(L.closure_conv_in(B, H, W, x.data_ptr(), self.p["w1"].data_ptr(), self.p["b1"].data_ptr(),
+        _chk(L.closure_conv_in(B, H, W, in_scale, x.data_ptr(), self.p["w1"].data_ptr(), self.p["b1"].data_ptr(),
                                z[1].data_ptr(), a[1].data_ptr(), _sp()))
         for l in range(2, 6):
             _ops.conv64(a[l - 1], self.wf[l], _ops.CLOSURE_EPI_FWD, bias=self.p[f"b{l}"], out_pad=a[l], out_z=z[l],
                         err=self.err)
         y = self.y[:B]
-        _chk(L.closure_conv_out(B, H, W, a[5].data_ptr(), self.p["w6"].data_ptr(), self.p["b6"].data_ptr(),
+        _chk(L.closure_conv_out(B, H, W, out_scale, a[5].data_ptr(), self.p["w6"].data_ptr(), self.p["b6"].data_ptr(),
                                 y.data_ptr(), _sp()))
         return y
 

@@ -1,0 +1,471 @@
+"""Learned-closure experiment: DNS -> filtered (theta, Pi) pairs -> CNN
+training -> coarse solves judged against the filtered DNS.
+
+    python -m pygsquig_b200.closure.experiment --out DIR [--calibrate]
+
+Physics (one configuration, all FP32 with IF-RK4): SQG alpha = 1 on
+[0, 2 pi)^2, ring forcing kf = 20, dk = 2, eps = 0.1 (host-drawn phases),
+CombinedDamping mu = 0.1 below kf/2 = 10 plus hyperviscosity nu = 1e-22,
+p = 8 at the DNS resolution N = 2048, dt = 1e-4.
+
+1. DNS.  Each run starts from a seeded random-phase field (spectrum
+   k^4 exp(-(k/10)^2), rms 1).  The large scales are spun up on a 512 grid
+   (hyperviscosity scaled so that nu k_max^8 matches the DNS), the state is
+   interpolated spectrally to 2048 and adjusted there before any sample is
+   taken.  Each run then has a recording window (training pairs every
+   ``pair_stride`` steps) and a later evaluation window (filtered spectra
+   every ``sample_dt``).
+2. Pairs.  theta_c = SpectralFilter(theta) on the 256 grid (|k| below its 2/3
+   radius); Pi = filter(NL_2048(theta)) - NL_256(theta_c), NL = the
+   dealiased advective tendency -mask fft2(u.grad theta); both to physical
+   space (library transforms).
+3. Training.  ClosureCNN on theta_c / sigma_theta -> Pi / sigma_pi, MSE,
+   Adam lr 1e-3, random D4 symmetry per batch (rotations; reflections with
+   theta, Pi -> -theta, -Pi, under which the equations are invariant).
+4. Evaluation.  From the filtered DNS state at the start of each run's
+   evaluation window the coarse N = 256 solve runs over the same span with
+   the closure, without it (same nu), and without it at a grid-scaled
+   hyperviscosity; time-mean shell spectra E(k) and energy transfer are
+   compared with the filtered DNS.  GPU time is CUDA-event time of the step
+   launches per unit of simulated time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import time
+from dataclasses import asdict, dataclass
+
+import numpy as np
+import torch
+
+from .. import _lib
+from .._plan import PlanKey, get_plan
+from ..core.grid import make_grid
+from ..core.solver import gSQGSolver
+from ..forcing.damping import CombinedDamping
+from ..forcing.ring_forcing import RingForcing
+from ..utils.fields import random_phase_field
+from .cnn import ClosureCNN
+from .model import ClosureSolver, SubgridClosure
+from .spectral import ShellSpectrum, SpectralFilter, interpolate_spectrum
+
+TWO_PI = 2 * math.pi
+
+
+@dataclass
+class Config:
+    N_dns: int = 2048
+    N_spin: int = 512
+    N_c: int = 256
+    alpha: float = 1.0
+    kf: float = 20.0
+    dk: float = 2.0
+    eps: float = 0.1
+    mu: float = 0.1
+    kf_damp: float = 20.0
+    nu: float = 1e-22
+    p: int = 8
+    dt: float = 1e-4
+    dt_spin: float = 2e-4
+    dt_c: float = 1e-3
+    runs: int = 8
+    seed0: int = 100
+    t_spin: float = 10.0
+    t_adjust: float = 0.5
+    pairs: int = 20000
+    pair_stride: int = 10
+    t_eval: float = 2.0
+    sample_dt: float = 0.01
+    epochs: int = 12
+    batch: int = 16
+    lr: float = 1e-3
+    val_frac: float = 0.05
+    train_seconds: float = 0.0  # > 0: stop training after this wall time
+
+
+def _nu_at(cfg: Config, N: int) -> float:
+    """Hyperviscosity giving the same nu k_max^p at the 2/3 radius of grid N."""
+    return cfg.nu * (cfg.N_dns / N) ** cfg.p
+
+
+class _Noise:
+    """Host-drawn ring phases (numpy default_rng), uploaded in chunks."""
+
+    def __init__(self, seed, n_ring, chunk=4096):
+        self.rng = np.random.default_rng(seed)
+        self.n_ring, self.chunk = n_ring, chunk
+        self.buf, self.pos = None, 0
+
+    def take(self, n) -> torch.Tensor:
+        if self.buf is None or self.pos + n > self.buf.shape[0]:
+            m = max(self.chunk, n)
+            self.buf = torch.from_numpy(self.rng.uniform(0, TWO_PI, size=(m, self.n_ring))).cuda()
+            self.pos = 0
+        out = self.buf[self.pos:self.pos + n]
+        self.pos += n
+        return out
+
+
+def _solver(cfg, N, nu, precision="float32"):
+    g = make_grid(N, TWO_PI)
+    s = gSQGSolver(g, cfg.alpha, 0.0, cfg.p, precision=precision, scheme="ifrk4")
+    damp = CombinedDamping(cfg.mu, cfg.kf_damp, nu, cfg.p)
+    ring = RingForcing(cfg.kf, cfg.dk, cfg.eps)
+    return g, s, damp, ring
+
+
+def _run_steps(s, st, n, dt, ring, damp, noise: _Noise, timer=None):
+    if timer is not None:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+    st = s.multistep(st, n, dt, forcing=ring, damping=damp, noise=noise.take(n))
+    if timer is not None:
+        e1.record()
+        timer.append((e0, e1))
+    return st
+
+
+def _elapsed_ms(timer) -> float:
+    torch.cuda.synchronize()
+    return float(sum(a.elapsed_time(b) for a, b in timer))
+
+
+class _Stats:
+    def __init__(self, n_shell):
+        self.E = torch.zeros(n_shell, dtype=torch.float64, device="cuda")
+        self.T = torch.zeros(n_shell, dtype=torch.float64, device="cuda")
+        self.n = 0
+
+    def add(self, E, T):
+        self.E += E
+        self.T += T
+        self.n += 1
+
+    def mean(self):
+        n = max(self.n, 1)
+        return (self.E / n).cpu().numpy(), (self.T / n).cpu().numpy()
+
+
+def generate(cfg: Config, log=print):
+    """DNS runs -> training pairs (device tensors), filtered-DNS statistics and
+    the coarse initial states of the evaluation windows."""
+    Nc = cfg.N_c
+    gs, s_spin, damp_spin, ring = _solver(cfg, cfg.N_spin, _nu_at(cfg, cfg.N_spin))
+    gf, s_dns, damp_dns, _ = _solver(cfg, cfg.N_dns, cfg.nu)
+    nl_f = get_plan(PlanKey(N=cfg.N_dns, L=TWO_PI, alpha=cfg.alpha, nu_p=0.0, p=cfg.p, precision="float32",
+                            role="aux"))
+    nl_c = get_plan(PlanKey(N=Nc, L=TWO_PI, alpha=cfg.alpha, nu_p=0.0, p=cfg.p, precision="float32", role="aux"))
+    filt = SpectralFilter(cfg.N_dns, Nc, TWO_PI)
+    shell = ShellSpectrum(Nc, TWO_PI, cfg.alpha)
+    n_ring_s = ring.n_modes(gs)
+    n_ring_f = ring.n_modes(gf)
+    per_run = cfg.pairs // cfg.runs
+    X = torch.empty((per_run * cfg.runs, Nc, Nc), dtype=torch.float32, device="cuda")
+    Y = torch.empty_like(X)
+    stats = _Stats(shell.n_shell)
+    run_E = []
+    ke = []
+    ics = []
+    t_dns = []
+    n_eval_steps = int(round(cfg.sample_dt / cfg.dt))
+    n_samples = int(round(cfg.t_eval / cfg.sample_dt))
+    spin_log = []
+    t0 = time.time()
+    for r in range(cfg.runs):
+        th0 = random_phase_field(cfg.N_spin, TWO_PI, lambda k: k**4 * np.exp(-((k / 10.0) ** 2)), cfg.seed0 + r)
+        st = s_spin.initialize(theta0=th0)
+        noise_s = _Noise(10_000 + r, n_ring_s)
+        n_spin = int(round(cfg.t_spin / cfg.dt_spin))
+        chunk = max(1, int(round(0.5 / cfg.dt_spin)))
+        done = 0
+        while done < n_spin:
+            n = min(chunk, n_spin - done)
+            st = _run_steps(s_spin, st, n, cfg.dt_spin, ring, damp_spin, noise_s)
+            done += n
+            if r == 0:
+                d = s_spin.get_diagnostics(st)
+                spin_log.append((done * cfg.dt_spin, d["kinetic_energy"], d["enstrophy"]))
+        thf = interpolate_spectrum(st["theta_hat"], cfg.N_dns)
+        st = {"theta_hat": thf, "time": st["time"], "step": st["step"]}
+        noise_f = _Noise(20_000 + r, n_ring_f)
+        st = _run_steps(s_dns, st, int(round(cfg.t_adjust / cfg.dt)), cfg.dt, ring, damp_dns, noise_f, t_dns)
+        # recording window: training pairs
+        for i in range(per_run):
+            st = _run_steps(s_dns, st, cfg.pair_stride, cfg.dt, ring, damp_dns, noise_f, t_dns)
+            th = st["theta_hat"]
+            thc = filt(th)
+            nlc_true = filt(nl_f.rhs(th))
+            pi_hat = nlc_true - nl_c.rhs(thc)
+            j = r * per_run + i
+            nl_c.to_physical(thc, out=X[j])
+            nl_c.to_physical(pi_hat, out=Y[j])
+        # evaluation window: filtered spectra and transfer
+        ics.append(filt(st["theta_hat"]).clone())
+        rs = _Stats(shell.n_shell)
+        for i in range(n_samples):
+            st = _run_steps(s_dns, st, n_eval_steps, cfg.dt, ring, damp_dns, noise_f, t_dns)
+            th = st["theta_hat"]
+            thc = filt(th)
+            E = shell.energy(thc)
+            T = shell.transfer(thc, filt(nl_f.rhs(th)))
+            stats.add(E, T)
+            rs.add(E, T)
+            if i % 20 == 0:
+                ke.append(s_dns.get_diagnostics(st)["kinetic_energy"])
+        run_E.append(rs.mean()[0])
+        log(f"[dns] run {r} done at {time.time() - t0:.0f} s, KE {ke[-1]:.4f}")
+    n_dns_steps = cfg.runs * (int(round(cfg.t_adjust / cfg.dt)) + per_run * cfg.pair_stride + n_samples * n_eval_steps)
+    ms = _elapsed_ms(t_dns)
+    dns = {
+        "E": stats.mean()[0], "T": stats.mean()[1], "run_E": np.array(run_E), "ke_mean": float(np.mean(ke)),
+        "ms_per_step": ms / n_dns_steps, "steps": n_dns_steps, "spin_log": spin_log,
+    }
+    return X, Y, ics, dns
+
+
+def train(cfg: Config, X, Y, log=print):
+    n = X.shape[0]
+    n_val = max(1, int(n * cfg.val_frac))
+    g = torch.Generator(device="cpu").manual_seed(1234)
+    perm = torch.randperm(n, generator=g).cuda()
+    val_idx, tr_idx = perm[:n_val], perm[n_val:]
+    sig_t = float(X[tr_idx[: min(2000, len(tr_idx))]].std().item())
+    sig_p = float(Y[tr_idx[: min(2000, len(tr_idx))]].std().item())
+    net = ClosureCNN(cfg.N_c, cfg.N_c, max_batch=cfg.batch, seed=0)
+    rng = np.random.default_rng(7)
+    B = cfg.batch
+    n_tr = len(tr_idx)
+    steps_per_epoch = n_tr // B
+    hist = []
+    t0 = time.time()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    it = 0
+    stop = False
+    for ep in range(cfg.epochs):
+        order = tr_idx[torch.randperm(n_tr, generator=g).cuda()]
+        acc = torch.zeros((), dtype=torch.float32, device="cuda")
+        for b in range(steps_per_epoch):
+            idx = order[b * B:(b + 1) * B]
+            xb = X.index_select(0, idx)
+            yb = Y.index_select(0, idx)
+            k = int(rng.integers(4))
+            if k:
+                xb = torch.rot90(xb, k, (1, 2))
+                yb = torch.rot90(yb, k, (1, 2))
+            if rng.integers(2):
+                xb = -xb.flip(2)
+                yb = -yb.flip(2)
+            xb = (xb * (1.0 / sig_t)).contiguous()
+            yb = (yb * (1.0 / sig_p)).contiguous()
+            acc += net.train_step(xb, yb, lr=cfg.lr)
+            it += 1
+            if cfg.train_seconds > 0 and time.time() - t0 > cfg.train_seconds:
+                stop = True
+                break
+        l = float(acc.item()) / max(b + 1, 1)
+        vl = validate(net, X, Y, val_idx, sig_t, sig_p)
+        hist.append({"epoch": ep, "train_mse": l, **vl, "wall_s": time.time() - t0})
+        log(f"[train] epoch {ep} mse {l:.4f} val {vl}")
+        if stop:
+            break
+    ev1.record()
+    torch.cuda.synchronize()
+    if net.errors():
+        raise RuntimeError("closure kernels reported a timed-out wait")
+    info = {"iters": it, "gpu_ms": ev0.elapsed_time(ev1), "sigma_theta": sig_t, "sigma_pi": sig_p, "history": hist,
+            "n_train": n_tr, "n_val": n_val}
+    return net, info, val_idx
+
+
+@torch.no_grad()
+def validate(net, X, Y, idx, sig_t, sig_p, max_n=256):
+    idx = idx[:max_n]
+    num = den = dot = ny = 0.0
+    B = net.maxB
+    for b in range(0, len(idx), B):
+        ii = idx[b:b + B]
+        x = (X.index_select(0, ii) / sig_t).contiguous()
+        y = Y.index_select(0, ii) / sig_p
+        p = net.forward(x)
+        num += float(((p - y) ** 2).sum().item())
+        den += float((y**2).sum().item())
+        dot += float((p * y).sum().item())
+        ny += float((p**2).sum().item())
+    return {"val_rel_mse": num / den, "val_corr": dot / math.sqrt(den * ny + 1e-300)}
+
+
+def evaluate(cfg: Config, closure: SubgridClosure, ics, dns, log=print):
+    Nc = cfg.N_c
+    shell = ShellSpectrum(Nc, TWO_PI, cfg.alpha)
+    nl_c = get_plan(PlanKey(N=Nc, L=TWO_PI, alpha=cfg.alpha, nu_p=0.0, p=cfg.p, precision="float32", role="aux"))
+    n_per = int(round(cfg.sample_dt / cfg.dt_c))
+    n_samples = int(round(cfg.t_eval / cfg.sample_dt))
+    variants = {
+        "closure": (cfg.nu, closure),
+        "no_closure": (cfg.nu, None),
+        "no_closure_grid_nu": (_nu_at(cfg, Nc), None),
+    }
+    out = {}
+    for name, (nu, clo) in variants.items():
+        g, s, damp, ring = _solver(cfg, Nc, nu)
+        runner = ClosureSolver(s, clo, damp, ring)
+        stats = _Stats(shell.n_shell)
+        timer = []
+        diverged = False
+        for r, ic in enumerate(ics):
+            st = {"theta_hat": ic.clone(), "time": 0.0, "step": 0}
+            noise = _Noise(30_000 + r, ring.n_modes(g))
+            for i in range(n_samples):
+                if clo is not None:
+                    st = runner.multistep(st, n_per, cfg.dt_c, noise.take(n_per), timer=timer)
+                else:
+                    st = _run_steps(s, st, n_per, cfg.dt_c, ring, damp, noise, timer)
+                th = st["theta_hat"]
+                tend = runner.tendency(th, nl_c)
+                stats.add(shell.energy(th), shell.transfer(th, tend))
+            if not bool(torch.isfinite(st["theta_hat"]).all().item()):
+                diverged = True
+        E, T = stats.mean()
+        steps = len(ics) * n_samples * n_per
+        ms = _elapsed_ms(timer)
+        out[name] = {"E": E, "T": T, "ms_per_step": ms / steps, "steps": steps, "diverged": diverged}
+        log(f"[eval] {name}: {ms / steps:.4f} ms/step diverged={diverged}")
+    if closure.errors():
+        raise RuntimeError("closure kernels reported a timed-out wait")
+    return out
+
+
+def time_cnn(net: ClosureCNN, reps: int = 20) -> dict:
+    """CUDA-event timing of one forward at batch 1 and one training step at
+    the network's batch; FLOPs of the four 64 -> 64 tensor-core layers
+    (2 x 9 x 64 x 64 per pixel each; forward once, backward twice)."""
+    H, W = net.H, net.W
+    x1 = torch.randn((1, H, W), device="cuda")
+    xb = torch.randn((net.maxB, H, W), device="cuda")
+    tb = torch.randn_like(xb)
+    save = [t.clone() for t in (net.flat, net.m, net.v)]
+    steps = net.step_count
+    for _ in range(3):
+        net.forward(x1)
+        net.train_step(xb, tb, lr=0.0)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    e[0].record()
+    for _ in range(reps):
+        net.forward(x1)
+    e[1].record()
+    for _ in range(reps):
+        net.train_step(xb, tb, lr=0.0)
+    e[2].record()
+    torch.cuda.synchronize()
+    for t, s in zip((net.flat, net.m, net.v), save):
+        t.copy_(s)
+    net.step_count = steps
+    net.refresh()
+    f_fwd = 4 * 2 * 9 * 64 * 64 * H * W
+    fwd = e[0].elapsed_time(e[1]) / reps
+    trn = e[1].elapsed_time(e[2]) / reps
+    return {"forward_ms_b1": fwd, "train_step_ms": trn, "batch": net.maxB,
+            "forward_tc_tflops": f_fwd / fwd * 1e-9, "train_tc_tflops": 3 * f_fwd * net.maxB / trn * 1e-9}
+
+
+def spectral_errors(E_model, E_ref, kmax):
+    k = np.arange(1, int(kmax) + 1)
+    rel = np.abs(E_model[k] - E_ref[k]) / E_ref[k]
+    return rel
+
+
+def flux(T):
+    return -np.cumsum(T)
+
+
+def report(cfg: Config, dns, train_info, ev, out_dir):
+    kf = int(cfg.kf)
+    u_rms = math.sqrt(2 * dns["ke_mean"])
+    t_eddy = (TWO_PI / cfg.kf) / u_rms
+    span = cfg.runs * cfg.t_eval
+    dns_ms_per_time = dns["ms_per_step"] / cfg.dt
+    rep = {
+        "config": asdict(cfg),
+        "eddy_time": {"definition": "(2 pi / kf) / u_rms, u_rms = sqrt(<u^2 + v^2>) of the DNS", "value": t_eddy,
+                      "u_rms": u_rms, "eval_span": span, "eval_span_eddy_times": span / t_eddy},
+        "dns": {"ms_per_step": dns["ms_per_step"], "ms_per_unit_time": dns_ms_per_time, "steps": dns["steps"]},
+        "training": {k: v for k, v in train_info.items()},
+        "shells": list(range(1, kf + 1)),
+        "E_dns": dns["E"][1:kf + 1].tolist(),
+        "flux_dns": flux(dns["T"])[1:kf + 1].tolist(),
+        "dns_run_spread_max": float(np.max(np.std(dns["run_E"][:, 1:kf + 1], axis=0) /
+                                           np.mean(dns["run_E"][:, 1:kf + 1], axis=0) / math.sqrt(cfg.runs))),
+        "spin_log": dns["spin_log"],
+        "models": {},
+    }
+    for name, m in ev.items():
+        rel = spectral_errors(m["E"], dns["E"], kf)
+        fl_m, fl_d = flux(m["T"]), flux(dns["T"])
+        nres = int((2.0 / 3.0) * cfg.N_c / 2)
+        rel_all = spectral_errors(m["E"], dns["E"], nres - 1)
+        rep["models"][name] = {
+            "ms_per_step": m["ms_per_step"],
+            "ms_per_unit_time": m["ms_per_step"] / cfg.dt_c,
+            "speedup_vs_dns": dns_ms_per_time / (m["ms_per_step"] / cfg.dt_c),
+            "E": m["E"][1:kf + 1].tolist(),
+            "rel_err_E": rel.tolist(),
+            "max_rel_err_E_k_le_kf": float(np.max(rel)),
+            "mean_rel_err_E_all_resolved": float(np.mean(rel_all)),
+            "max_rel_err_E_all_resolved": float(np.max(rel_all)),
+            "flux": fl_m[1:kf + 1].tolist(),
+            "flux_rel_err_at_kf": float(abs(fl_m[kf] - fl_d[kf]) / (abs(fl_d[kf]) + 1e-300)),
+            "diverged": m["diverged"],
+        }
+    os.makedirs(out_dir, exist_ok=True)
+    with open(os.path.join(out_dir, "closure_report.json"), "w") as f:
+        json.dump(rep, f, indent=1, default=float)
+    return rep
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default="closure_out")
+    ap.add_argument("--calibrate", action="store_true", help="one short run of each stage (timings, statistics)")
+    ap.add_argument("--set", nargs="*", default=[], help="Config overrides name=value")
+    a = ap.parse_args(argv)
+    cfg = Config()
+    if a.calibrate:
+        cfg = Config(runs=1, pairs=400, t_spin=10.0, t_adjust=0.2, t_eval=0.5, epochs=2, pair_stride=10)
+    for kv in a.set:
+        k, v = kv.split("=")
+        setattr(cfg, k, type(getattr(cfg, k))(v))
+    torch.cuda.set_device(0)
+    from ..build import build
+
+    build()
+    log = lambda *m: print(*m, flush=True)  # noqa: E731
+    t0 = time.time()
+    X, Y, ics, dns = generate(cfg, log)
+    log(f"[dns] {dns['ms_per_step']:.4f} ms/step, KE {dns['ke_mean']:.4f}, wall {time.time() - t0:.0f} s")
+    net, tinfo, val_idx = train(cfg, X, Y, log)
+    tinfo["cnn_timing"] = time_cnn(net)
+    log(f"[train] cnn timing {tinfo['cnn_timing']}")
+    closure = SubgridClosure(net, cfg.N_c, TWO_PI, tinfo["sigma_theta"], tinfo["sigma_pi"])
+    os.makedirs(a.out, exist_ok=True)
+    closure.save(os.path.join(a.out, "closure_weights.npz"), config=asdict(cfg))
+    ev = evaluate(cfg, closure, ics, dns, log)
+    rep = report(cfg, dns, tinfo, ev, a.out)
+    # small fixtures: validation pairs, one coarse initial state, the DNS spectrum
+    vi = val_idx[:4]
+    np.savez_compressed(os.path.join(a.out, "closure_fixture.npz"), theta=X[vi].cpu().numpy(),
+                        pi=Y[vi].cpu().numpy(), ic=ics[-1].cpu().numpy(), E_dns=dns["E"],
+                        T_dns=dns["T"])
+    summ = {k: {kk: v[kk] for kk in ("max_rel_err_E_k_le_kf", "speedup_vs_dns", "mean_rel_err_E_all_resolved",
+                                     "diverged")} for k, v in rep["models"].items()}
+    log(json.dumps({"eddy_time": rep["eddy_time"], "models": summ}))
+    log(f"[done] wall {time.time() - t0:.0f} s")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

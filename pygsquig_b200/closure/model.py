@@ -1,0 +1,167 @@
+"""The learned subgrid closure as a forcing term of the coarse solve, and a
+coarse solver that replays its step (closure included) as a CUDA graph.
+
+The closure models the nonlinear term the coarse grid cannot carry,
+    Pi = filter(-mask fft2(u.grad theta)) - (-mask_c fft2(u_c.grad theta_c)),
+with theta_c = filter(theta) (the sharp filter of spectral.SpectralFilter).
+It is evaluated on every RK stage input: theta_s -> physical theta (library
+transform) -> CNN (library kernels, BF16 tensor cores) -> spectrum (library
+transform) -> restricted to the coarse dealiased disk and added to that
+stage's right-hand side, exactly where the solver adds any forcing term.
+"""
+
+from __future__ import annotations
+
+import math
+from typing import Optional
+
+import numpy as np
+import torch
+
+from .. import _lib
+from .._plan import PlanKey, get_plan
+from ..exceptions import NumericalError
+from ..forcing.damping import CombinedDamping
+from ..forcing.ring_forcing import RingForcing
+from .cnn import ClosureCNN
+from .spectral import _kmag
+
+
+class SubgridClosure:
+    """forcing(theta_hat) -> closure spectrum (a term for gSQGSolver.step).
+
+    ``sigma_theta`` / ``sigma_pi`` are the training normalisation: the CNN
+    maps theta / sigma_theta to Pi / sigma_pi.
+    """
+
+    def __init__(self, net: ClosureCNN, N: int, L: float, sigma_theta: float, sigma_pi: float,
+                 k_cut: Optional[float] = None, precision: str = "float32"):
+        if net.H != N or net.W != N:
+            raise ValueError("the network was built for another grid")
+        self.net, self.N, self.L = net, N, L
+        self.sigma_theta, self.sigma_pi = float(sigma_theta), float(sigma_pi)
+        self.plan = get_plan(PlanKey(N=N, L=L, alpha=0.0, nu_p=0.0, p=8, precision=precision, role="closure"))
+        dev = self.plan.device
+        self.k_cut = (2.0 / 3.0) * math.pi * N / L if k_cut is None else k_cut
+        self.mult = (_kmag(N, L, dev) < self.k_cut).to(self.plan.cdtype)
+        self.phys = torch.empty((N, N), dtype=self.plan.rdtype, device=dev)
+        self.x = torch.empty((1, N, N), dtype=torch.float32, device=dev)
+        self.spec = torch.empty((N, N), dtype=self.plan.cdtype, device=dev)
+        self.yspec_in = torch.empty((N, N), dtype=self.plan.rdtype, device=dev)
+
+    def physical(self, theta_hat: torch.Tensor, normalised: bool = False) -> torch.Tensor:
+        """CNN output Pi (FP32 [N, N]) for a coarse spectrum; the
+        normalisation is folded into the first and last layers."""
+        if self.plan.rdtype == torch.float32:
+            self.plan.to_physical(theta_hat, out=self.x[0])
+        else:
+            self.plan.to_physical(theta_hat, out=self.phys)
+            self.x[0].copy_(self.phys)
+        return self.net.forward(self.x, in_scale=1.0 / self.sigma_theta,
+                                out_scale=1.0 if normalised else self.sigma_pi)[0]
+
+    def __call__(self, theta_hat: torch.Tensor, **kwargs) -> torch.Tensor:
+        y = self.physical(theta_hat)
+        if self.yspec_in.dtype != y.dtype:
+            self.yspec_in.copy_(y)
+            y = self.yspec_in
+        self.plan.to_spectral(y, out=self.spec)
+        return self.spec * self.mult
+
+    def errors(self) -> int:
+        return self.net.errors()
+
+    # ---- persistence ----
+    def save(self, path: str, **meta) -> None:
+        d = {k: v.numpy() for k, v in self.net.state_dict().items()}
+        np.savez(path, sigma_theta=self.sigma_theta, sigma_pi=self.sigma_pi, N=self.N, L=self.L, k_cut=self.k_cut,
+                 meta=np.array(repr(meta)), **d)
+
+    @classmethod
+    def load(cls, path: str, max_batch: int = 1, precision: str = "float32") -> "SubgridClosure":
+        z = np.load(path)
+        N = int(z["N"])
+        net = ClosureCNN(N, N, max_batch=max_batch)
+        net.load_state_dict({k: torch.as_tensor(z[k]) for k, _ in ClosureCNN.SHAPES})
+        return cls(net, N, float(z["L"]), float(z["sigma_theta"]), float(z["sigma_pi"]), float(z["k_cut"]),
+                   precision)
+
+
+class ClosureSolver:
+    """Coarse gSQG solve with fused ring forcing / damping plus a learned
+    closure on every RK stage; ``multistep`` captures one step (4 closure
+    evaluations and 4 fused stages) in a CUDA graph and replays it."""
+
+    def __init__(self, solver, closure: Optional[SubgridClosure], damping: Optional[CombinedDamping] = None,
+                 ring: Optional[RingForcing] = None):
+        if solver.scheme != "ifrk4" and solver.scheme != "explicit":
+            raise ValueError("unknown scheme")
+        self.solver, self.closure, self.damping, self.ring = solver, closure, damping, ring
+        self.pl = solver.plan(damping, ring)
+        N = solver.grid.N
+        dev = self.pl.device
+        self.th_a = torch.zeros((N, N), dtype=self.pl.cdtype, device=dev)
+        self.th_b = torch.zeros_like(self.th_a)
+        self.ph = torch.zeros(max(self.pl.n_ring, 1), dtype=torch.float64, device=dev)
+        self.graph = None
+        self.graph_dt = None
+
+    def _body(self, dt):
+        pl = self.pl
+        stage_buf = pl.buffer(_lib.SQG_BUF_STAGE, self.th_a.dtype, self.th_a.shape)
+        ph = self.ph if self.ring is not None else None
+        pl.stage_begin(self.th_a)
+        for s in range(1, 5):
+            th_s = self.th_a if s == 1 else stage_buf
+            extra = self.closure(th_s) if self.closure is not None else None
+            pl.stage(s, self.th_a, self.th_b, dt, extra, ph)
+        self.th_a.copy_(self.th_b)
+
+    def _capture(self, dt):
+        cur = torch.cuda.current_stream()
+        side = torch.cuda.Stream()
+        side.wait_stream(cur)
+        save = self.th_a.clone()
+        with torch.cuda.stream(side):
+            self._body(dt)  # warm-up outside the capture (kernel attributes, allocator)
+        cur.wait_stream(side)
+        self.th_a.copy_(save)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, capture_error_mode="thread_local"):
+            self._body(dt)
+        self.graph, self.graph_dt = g, dt
+
+    def multistep(self, state: dict, n_steps: int, dt: float, noise: Optional[torch.Tensor] = None,
+                  timer: Optional[list] = None) -> dict:
+        """n_steps steps; ``noise``: device float64 [n_steps, n_ring] ring
+        phases.  ``timer`` (a list) receives (start, end) CUDA events around
+        the replays."""
+        if self.ring is not None and (noise is None or noise.shape[0] < n_steps):
+            raise ValueError("ring forcing needs noise of shape (n_steps, n_ring)")
+        self.th_a.copy_(self.pl.check_spectrum(state["theta_hat"]))
+        if self.graph is None or self.graph_dt != dt:
+            self._capture(dt)
+            self.th_a.copy_(self.pl.check_spectrum(state["theta_hat"]))
+        ev = None
+        if timer is not None:
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            ev[0].record()
+        for i in range(n_steps):
+            if self.ring is not None:
+                self.ph.copy_(noise[i])
+            self.graph.replay()
+        if ev is not None:
+            ev[1].record()
+            timer.append(ev)
+        if self.solver.check_finite and self.pl.check_status():
+            raise NumericalError("non-finite values in theta_hat")
+        return {"theta_hat": self.th_a.clone(), "time": state["time"] + n_steps * dt,
+                "step": state["step"] + n_steps}
+
+    def tendency(self, theta_hat: torch.Tensor, aux_plan) -> torch.Tensor:
+        """Resolved nonlinear tendency plus the closure term (for transfer
+        spectra); ``aux_plan``: an inviscid plan of the coarse grid."""
+        t = aux_plan.rhs(theta_hat)
+        if self.closure is not None:
+            t = t + self.closure(theta_hat)
+        return t

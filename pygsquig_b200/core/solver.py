@@ -11,7 +11,8 @@ Forcing / damping protocol (solver.py:150-214).  ``step`` accepts:
   callable ``damping(theta_hat, **kwargs)`` returning a spectrum;
 * ``forcing``: ``RingForcing.bind(key, dt, grid)`` (fused), a ``RingForcing``
   together with ``key=`` phases in kwargs (fused), or any callable
-  ``forcing(theta_hat, **kwargs)``.
+  ``forcing(theta_hat, **kwargs)``; or a list of such terms (their sum, e.g.
+  a bound ring forcing plus a learned subgrid closure).
 
 Callables the kernels do not carry are evaluated by the host on every RK
 stage input and added to that stage's right-hand side, exactly where the
@@ -135,14 +136,18 @@ class gSQGSolver:
             damp = damping
         elif damping is not None:
             generic.append(damping)
-        if isinstance(forcing, BoundRingForcing):
-            ring, phases_key = forcing.ring, forcing.key
-        elif isinstance(forcing, RingForcing):
-            if "key" not in kwargs:
-                raise TypeError("RingForcing passed directly needs key=<phases> (or use ring.bind(key, dt, grid))")
-            ring, phases_key = forcing, kwargs["key"]
-        elif forcing is not None:
-            generic.append(forcing)
+        terms = list(forcing) if isinstance(forcing, (list, tuple)) else ([] if forcing is None else [forcing])
+        for f in terms:
+            if isinstance(f, (BoundRingForcing, RingForcing)) and ring is not None:
+                raise ValueError("at most one RingForcing per step")
+            if isinstance(f, BoundRingForcing):
+                ring, phases_key = f.ring, f.key
+            elif isinstance(f, RingForcing):
+                if "key" not in kwargs:
+                    raise TypeError("RingForcing passed directly needs key=<phases> (or use ring.bind(key, dt, grid))")
+                ring, phases_key = f, kwargs["key"]
+            else:
+                generic.append(f)
         return damp, ring, phases_key, generic
 
     def step(self, state: State, dt: float, forcing: Optional[Callable] = None, damping: Optional[Callable] = None,
@@ -177,12 +182,15 @@ class gSQGSolver:
         (n_steps, n_ring) (one row of ring phases per step).  Without ring
         forcing the step is captured once in a CUDA graph and replayed.
         """
-        if isinstance(forcing, BoundRingForcing):
-            forcing = forcing.ring
-        damp, ring, _, generic = self._classify(forcing, damping, dict(kwargs, key=None))
+        terms = list(forcing) if isinstance(forcing, (list, tuple)) else ([] if forcing is None else [forcing])
+        terms = [f.ring if isinstance(f, BoundRingForcing) else f for f in terms]
+        damp, ring, _, generic = self._classify(terms, damping, dict(kwargs, key=None))
         if generic:
+            gen_f = [f for f in terms if not isinstance(f, RingForcing)]
             for i in range(n_steps):
-                f = forcing if ring is None else ring.bind(None if noise is None else noise[i], dt, self.grid)
+                f = list(gen_f)
+                if ring is not None:
+                    f.append(ring.bind(None if noise is None else noise[i], dt, self.grid))
                 state = self.step(state, dt, forcing=f, damping=damping, **kwargs)
             return state
         pl = self.plan(damp, ring)

@@ -3,14 +3,20 @@
 //
 // Implicit GEMM: M = 128 pixels of one image row (a tile), N = 64 output
 // channels, K = 9 taps x 64 input channels (one 64-wide K block per tap).
-// Activations are NHWC BF16 with a one-pixel circular halo, so the A block of
-// tap (dy, dx) is 128 consecutive pixel rows of 128 bytes: one TMA box
-// (128B-swizzled) straight from the halo'd tensor.  The weights of the 9 taps
-// stay in shared memory for the life of the persistent CTA.
+// Activations are NHWC BF16 with a one-pixel circular halo.  For each of the
+// three input rows a tile needs, one TMA box brings 130 pixels (the tile and
+// its two neighbours) into shared memory in the unswizzled K-major core-matrix
+// layout (8 pixels x 16 bytes per core matrix, channel groups 130 x 16 bytes
+// apart), so the A operand of tap (dy, dx) is the slab of row dy read from
+// pixel dx: a 16-byte shift of the descriptor start.  Each activation byte is
+// fetched three times instead of nine.  The weights of the 9 taps stay in
+// shared memory (128B-swizzled, K-major) for the life of the persistent CTA.
 //
-// Warp roles (6 warps): warp 0 issues TMA loads, warp 1 allocates TMEM and
-// issues the MMAs (one elected thread), warps 2..5 read the FP32 accumulators
-// from TMEM (tcgen05.ld, one lane quarter each) and run the epilogue.  Two
+// Warp roles (10 warps): warp 0 issues TMA loads, warp 1 allocates TMEM and
+// issues the MMAs (one elected thread), warps 2..9 read the FP32 accumulators
+// from TMEM (tcgen05.ld; warp w may read lane quarter w % 4, so two warps
+// share each quarter and take 32 of the 64 columns each) and run the
+// epilogue.  Two
 // TMEM accumulators alternate so the epilogue of tile i overlaps the MMAs of
 // tile i+1.  Every mbarrier wait is bounded: on time-out the kernel records
 // an error flag and the roles drain and return.
@@ -40,9 +46,14 @@ int cfail(int code, const std::string& m) {
 constexpr int kStages = 6;
 constexpr int kTileM = 128;
 constexpr int kC = 64;
-constexpr int kABytes = kTileM * kC * 2;  // 16 KB per tap slice
+constexpr int kSlabPix = kTileM + 2;       // pixels of one input-row slab
+constexpr int kSlabBytes = kSlabPix * kC * 2;  // 16640 B
+// Guard band after the slabs: every descriptor address stays inside the
+// allocation even if a stride were misread.
+constexpr int kSmemGuard = 32768;
 constexpr int kBBytes = kC * kC * 2;      // 8 KB per tap
-constexpr int kThreads = 192;
+constexpr int kThreads = 320;
+constexpr int kEpiWarps = 8;
 constexpr uint32_t kWaitLimit = 1u << 26;
 
 // ---- PTX helpers ------------------------------------------------------------
@@ -85,6 +96,20 @@ __device__ __forceinline__ uint64_t sw128_desc(const void* smem_tile) {
   const uint64_t start = (smem_u32(smem_tile) >> 4) & 0x3FFF;
   const uint64_t lbo = 1, sbo = 1024 >> 4;
   return start | (lbo << 16) | (sbo << 32) | (1ull << 46) | (2ull << 61);
+}
+// K-major, no swizzle: core matrices of 8 pixels x 16 B (128 B contiguous),
+// next 8 pixels 128 B away (SBO), next 8 channels one slab row-group away (LBO)
+__device__ __forceinline__ uint64_t slab_desc(const void* slab) {
+  const uint64_t start = (smem_u32(slab) >> 4) & 0x3FFF;
+  const uint64_t lbo = (kSlabPix * 16) >> 4, sbo = 128 >> 4;
+  return start | (lbo << 16) | (sbo << 32) | (1ull << 46);
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+      : "memory");
 }
 // BF16 x BF16 -> FP32, K-major A and B, M = 128, N = 64
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
@@ -130,10 +155,10 @@ struct ConvArgs {
   unsigned* err;
 };
 
-// Writes the 64 BF16 values of pixel (b, y, x) to the halo'd tensor,
-// including its circular copies on the halo.
-__device__ __forceinline__ void store_halo(__nv_bfloat16* out, int H, int W, int b, int y, int x,
-                                           const uint4 (&v)[8]) {
+// Writes 32 BF16 channels (from channel c0) of pixel (b, y, x) to the halo'd
+// tensor, including their circular copies on the halo.
+__device__ __forceinline__ void store_halo(__nv_bfloat16* out, int H, int W, int b, int y, int x, int c0,
+                                           const uint4 (&v)[4]) {
   const int Wp = W + 2, Hp = H + 2;
   int ys[2] = {y + 1, -1}, xs[2] = {x + 1, -1};
   if (y == 0) ys[1] = H + 1;
@@ -144,9 +169,9 @@ __device__ __forceinline__ void store_halo(__nv_bfloat16* out, int H, int W, int
     if (ys[a] < 0) continue;
     for (int c = 0; c < 2; ++c) {
       if (xs[c] < 0) continue;
-      uint4* dst = reinterpret_cast<uint4*>(out + (((size_t)b * Hp + ys[a]) * Wp + xs[c]) * kC);
+      uint4* dst = reinterpret_cast<uint4*>(out + (((size_t)b * Hp + ys[a]) * Wp + xs[c]) * kC + c0);
 #pragma unroll
-      for (int i = 0; i < 8; ++i) dst[i] = v[i];
+      for (int i = 0; i < 4; ++i) dst[i] = v[i];
     }
   }
 }
@@ -157,8 +182,8 @@ k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CU
   // 1024-byte aligned carve-up
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* sB = base;                          // 9 x 8 KB weights
-  unsigned char* sA = base + 9 * kBBytes;            // kStages x 16 KB activations
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sA + kStages * kABytes);
+  unsigned char* sA = base + 9 * kBBytes;            // kStages x 16640 B row slabs
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sA + kStages * kSlabBytes + kSmemGuard);
   uint64_t* full = bars;                 // [kStages]
   uint64_t* empty = bars + kStages;      // [kStages]
   uint64_t* acc_full = bars + 2 * kStages;   // [2]
@@ -177,7 +202,7 @@ k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CU
     }
     for (int i = 0; i < 2; ++i) {
       mbar_init(&acc_full[i], 1);
-      mbar_init(&acc_empty[i], 4);  // one arrive per epilogue warp
+      mbar_init(&acc_empty[i], kEpiWarps);  // one arrive per epilogue warp
     }
     mbar_init(wbar, 1);
     mbar_init(wbar + 2, 1);  // drain barrier of the error path
@@ -204,14 +229,14 @@ k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CU
         const int xt = tile % tiles_per_row;
         const int rowi = tile / tiles_per_row;
         const int y = rowi % a.H, b = rowi / a.H;
-        for (int t = 0; t < 9 && ok; ++t, ++it) {
+        for (int dy = 0; dy < 3 && ok; ++dy, ++it) {
           const int s = it % kStages;
           const uint32_t ph = (it / kStages) & 1;
           if (it >= kStages && !mbar_wait(&empty[s], ph ^ 1)) { ok = false; break; }
-          const int dy = t / 3 - 1, dx = t % 3 - 1;
-          const int q = (b * (a.H + 2) + (y + 1 + dy)) * (a.W + 2) + (xt * kTileM + 1 + dx);
-          mbar_expect_tx(&full[s], kABytes);
-          tma_load_2d(sA + s * kABytes, &act_map, &full[s], 0, q);
+          // padded row y + dy, padded columns xt*128 .. xt*128 + 129
+          const int q = (b * (a.H + 2) + (y + dy)) * (a.W + 2) + xt * kTileM;
+          mbar_expect_tx(&full[s], kSlabBytes);
+          tma_load_3d(sA + s * kSlabBytes, &act_map, &full[s], 0, q, 0);
         }
       }
       if (!ok) {
@@ -231,17 +256,21 @@ k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CU
         if (tcount >= 2 && !mbar_wait(&acc_empty[acc], aph ^ 1)) { ok = false; break; }
         tc_fence_after();
         const uint32_t d = tmem + acc * 64;
-        for (int t = 0; t < 9 && ok; ++t, ++it) {
+        for (int dy = 0; dy < 3 && ok; ++dy, ++it) {
           const int s = it % kStages;
           const uint32_t ph = (it / kStages) & 1;
           if (!mbar_wait(&full[s], ph)) { ok = false; break; }
           tc_fence_after();
-          const uint64_t ad = sw128_desc(sA + s * kABytes);
-          const uint64_t bd = sw128_desc(sB + t * kBBytes);
+          const uint64_t ad = slab_desc(sA + s * kSlabBytes);
 #pragma unroll
-          for (int k = 0; k < 4; ++k)  // K = 16 per MMA: 32 bytes along the 128-byte row
-            umma(d, ad + 2 * k, bd + 2 * k, (t > 0 || k > 0) ? 1u : 0u);
-          umma_commit(&empty[s]);  // frees the slot when these MMAs complete
+          for (int dx = 0; dx < 3; ++dx) {
+            const int t = 3 * dy + dx;
+            const uint64_t bd = sw128_desc(sB + t * kBBytes);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)  // K = 16 channels: two core matrices (2 LBO) per MMA
+              umma(d, ad + dx + 2 * k * kSlabPix, bd + 2 * k, (t > 0 || k > 0) ? 1u : 0u);
+          }
+          umma_commit(&empty[s]);  // frees the slab when these MMAs complete
         }
         umma_commit(&acc_full[acc]);
       }
@@ -253,25 +282,26 @@ k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CU
       }
     }
   } else {
-    // ---------------- epilogue (warps 2..5) ----------------
+    // ---------------- epilogue (warps 2..9) ----------------
     const int quarter = warp & 3;  // TMEM lane quarter this warp may access
+    const int c0 = ((warp - 2) >> 2) * 32;  // its 32 accumulator columns
     const int row = quarter * 32 + lane;
+    float bz[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) bz[i] = (a.mode == CLOSURE_EPI_DGRAD) ? 0.f : a.bias[c0 + i];
     int tcount = 0;
     for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x, ++tcount) {
       const int acc = tcount & 1;
       const uint32_t aph = (tcount >> 1) & 1;
       if (!mbar_wait(&acc_full[acc], aph)) { ok = false; break; }
       tc_fence_after();
-      float v[64];
+      float v[32];
       uint32_t r[32];
-      const uint32_t taddr = tmem + acc * 64 + ((uint32_t)(quarter * 32) << 16);
+      const uint32_t taddr = tmem + acc * 64 + c0 + ((uint32_t)(quarter * 32) << 16);
       TC_LD32(taddr, r);
-#pragma unroll
-      for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-      TC_LD32(taddr + 32, r);
-#pragma unroll
-      for (int i = 0; i < 32; ++i) v[32 + i] = __uint_as_float(r[i]);
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+      for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]) + bz[i];
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&acc_empty[acc]);
@@ -282,41 +312,37 @@ k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CU
       const int x = xt * kTileM + row;
       const size_t pix = ((size_t)b * a.H + y) * a.W + x;
       if (a.mode == CLOSURE_EPI_LIN) {
-        float4* o = reinterpret_cast<float4*>(a.out_f32 + pix * kC);
+        float4* o = reinterpret_cast<float4*>(a.out_f32 + pix * kC + c0);
 #pragma unroll
-        for (int i = 0; i < 16; ++i)
-          o[i] = make_float4(v[4 * i] + a.bias[4 * i], v[4 * i + 1] + a.bias[4 * i + 1],
-                             v[4 * i + 2] + a.bias[4 * i + 2], v[4 * i + 3] + a.bias[4 * i + 3]);
+        for (int i = 0; i < 8; ++i) o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
         continue;
       }
-      uint4 packed[8];
+      uint4 packed[4];
       if (a.mode == CLOSURE_EPI_FWD) {
-        uint4 zp[8];
+        uint4 zp[4];
 #pragma unroll
-        for (int i = 0; i < 32; ++i) {
-          const float z0 = v[2 * i] + a.bias[2 * i], z1 = v[2 * i + 1] + a.bias[2 * i + 1];
-          const __nv_bfloat162 zb = __floats2bfloat162_rn(z0, z1);
+        for (int i = 0; i < 16; ++i) {
+          const __nv_bfloat162 zb = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
           const float2 zr = __bfloat1622float2(zb);  // the stored pre-activation
-          const __nv_bfloat162 g = __floats2bfloat162_rn(gelu(zr.x), gelu(zr.y));
           reinterpret_cast<__nv_bfloat162*>(zp)[i] = zb;
-          reinterpret_cast<__nv_bfloat162*>(packed)[i] = g;
+          reinterpret_cast<__nv_bfloat162*>(packed)[i] = __floats2bfloat162_rn(gelu(zr.x), gelu(zr.y));
         }
-        uint4* oz = reinterpret_cast<uint4*>(a.out_z + pix * kC);
+        uint4* oz = reinterpret_cast<uint4*>(a.out_z + pix * kC + c0);
 #pragma unroll
-        for (int i = 0; i < 8; ++i) oz[i] = zp[i];
+        for (int i = 0; i < 4; ++i) oz[i] = zp[i];
       } else {  // DGRAD
-        const uint4* zsrc = reinterpret_cast<const uint4*>(a.zprev + pix * kC);
-        uint4 zq[8];
+        const uint4* zsrc = reinterpret_cast<const uint4*>(a.zprev + pix * kC + c0);
+        uint4 zq[4];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) zq[i] = zsrc[i];
+        for (int i = 0; i < 4; ++i) zq[i] = zsrc[i];
 #pragma unroll
-        for (int i = 0; i < 32; ++i) {
+        for (int i = 0; i < 16; ++i) {
           const float2 z = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(zq)[i]);
           reinterpret_cast<__nv_bfloat162*>(packed)[i] =
               __floats2bfloat162_rn(v[2 * i] * gelu_grad(z.x), v[2 * i + 1] * gelu_grad(z.y));
         }
       }
-      store_halo(a.out_pad, a.H, a.W, b, y, x, packed);
+      store_halo(a.out_pad, a.H, a.W, b, y, x, c0, packed);
     }
     if (!ok) atomicOr(a.err, 4u);
   }
@@ -336,6 +362,7 @@ k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CU
 // range of pixel blocks and writes its partial sums; k_wgrad_reduce adds the
 // partials in a fixed order.
 constexpr int kWStages = 2;
+constexpr int kWThreads = 192;  // TMA warp, MMA warp, 4 epilogue warps
 constexpr int kWSlot = 64 * kC * 2;             // 8 KB: 64 pixel rows x 64 channels
 constexpr int kWStageBytes = 11 * kWSlot;       // 10 activation slots + 1 gradient slot
 // MN-major A/B, BF16 -> FP32, M = 128, N = 64
@@ -363,7 +390,7 @@ struct WgradArgs {
   unsigned* err;
 };
 
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kWThreads, 1)
 k_wgrad64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CUtensorMap g_map, WgradArgs a) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -521,7 +548,22 @@ bool make_map(CUtensorMap* m, const void* ptr, uint64_t rows, uint32_t box_rows)
            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-constexpr size_t kSmemBytes = 1024 + 9 * kBBytes + kStages * kABytes + 256;
+// Halo'd activations as [rows][8 channel groups][8 channels]: box = 8
+// channels x 130 pixels x 8 groups, written unswizzled, channel group
+// outermost (the slab layout of slab_desc).
+bool make_slab_map(CUtensorMap* m, const void* ptr, uint64_t rows) {
+  PFN_encodeTiled f = encode_fn();
+  if (!f) return false;
+  cuuint64_t dims[3] = {8, rows, 8};
+  cuuint64_t strides[2] = {kC * 2, 16};
+  cuuint32_t box[3] = {8, (cuuint32_t)kSlabPix, 8};
+  cuuint32_t estr[3] = {1, 1, 1};
+  return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(ptr), dims, strides, box, estr,
+           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+constexpr size_t kSmemBytes = 1024 + 9 * kBBytes + kStages * kSlabBytes + kSmemGuard + 256;
 
 }  // namespace
 
@@ -541,7 +583,7 @@ int closure_conv64(int32_t B, int32_t H, int32_t W, int32_t mode, const void* ac
   if (mode == CLOSURE_EPI_LIN && (!bias || !out_f32)) return cfail(1, "closure_conv64: LIN needs bias, out_f32");
   CUtensorMap amap, wmap;
   const uint64_t prows = (uint64_t)B * (H + 2) * (W + 2);
-  if (!make_map(&amap, act_pad, prows, kTileM) || !make_map(&wmap, weights, 9 * kC, kC))
+  if (!make_slab_map(&amap, act_pad, prows) || !make_map(&wmap, weights, 9 * kC, kC))
     return cfail(2, "closure_conv64: tensor map encoding failed");
   static bool attr = false;
   if (!attr) {
@@ -583,7 +625,7 @@ int closure_wgrad64(int32_t B, int32_t H, int32_t W, const void* act_pad, const 
   WgradArgs a;
   a.B = B; a.H = H; a.W = W; a.partials = partials; a.err = err;
   cudaStream_t st = (cudaStream_t)stream;
-  k_wgrad64<<<nparts, kThreads, smem, st>>>(amap, gmap, a);
+  k_wgrad64<<<nparts, kWThreads, smem, st>>>(amap, gmap, a);
   k_wgrad_reduce<<<(9 * 4096 + 255) / 256, 256, 0, st>>>(partials, nparts, dw);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cfail(2, std::string("closure_wgrad64 launch: ") + cudaGetErrorString(e));

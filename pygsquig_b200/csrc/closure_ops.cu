@@ -31,170 +31,248 @@ __device__ __forceinline__ size_t padidx(int b, int y, int x, int H, int W) {
   return ((size_t)b * (H + 2) + (y + 1)) * (W + 2) + (x + 1);
 }
 
-// Writes the 64 BF16 channels of interior pixel (b, y, x) and its halo copies.
-__device__ __forceinline__ void put_halo(__nv_bfloat16* out, int H, int W, int b, int y, int x, const float* v) {
-  int ys[2] = {y + 1, -1}, xs[2] = {x + 1, -1};
-  if (y == 0) ys[1] = H + 1;
-  if (y == H - 1) ys[1] = 0;
-  if (x == 0) xs[1] = W + 1;
-  if (x == W - 1) xs[1] = 0;
-  uint4 pk[8];
+// Work item of one warp: 32 consecutive pixels of one image row (W is a
+// multiple of 32); lane l owns the channel pair (2l, 2l + 1), so every
+// per-pixel access of a 64-channel tensor is one coalesced 128-byte row.
+constexpr int kChunk = 32;
+constexpr int kWarps = 8;  // warps per block of the chunked kernels
+
+struct Chunk {
+  int b, y, x0;
+  size_t p0;  // linear index of the first pixel
+};
+__device__ __forceinline__ Chunk chunk_of(size_t ch, int H, int W) {
+  Chunk c;
+  c.p0 = ch * kChunk;
+  c.x0 = (int)(c.p0 % W);
+  const size_t r = c.p0 / W;
+  c.y = (int)(r % H);
+  c.b = (int)(r / H);
+  return c;
+}
+
+// Rows y-1, y, y+1 (circular) of a scalar field, columns x0-1 .. x0+32, into s[3][34].
+__device__ __forceinline__ void stage_rows(float (*s)[34], const float* __restrict__ f, int H, int W, const Chunk& c,
+                                           int lane) {
 #pragma unroll
-  for (int i = 0; i < 32; ++i) reinterpret_cast<__nv_bfloat162*>(pk)[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-  for (int a = 0; a < 2; ++a) {
-    if (ys[a] < 0) continue;
-    for (int c = 0; c < 2; ++c) {
-      if (xs[c] < 0) continue;
-      uint4* d = reinterpret_cast<uint4*>(out + (((size_t)b * (H + 2) + ys[a]) * (W + 2) + xs[c]) * 64);
-#pragma unroll
-      for (int i = 0; i < 8; ++i) d[i] = pk[i];
-    }
+  for (int r = 0; r < 3; ++r) {
+    const float* row = f + ((size_t)c.b * H + wrap(c.y + r - 1, H)) * W;
+    s[r][lane + 1] = row[c.x0 + lane];
+    if (lane == 0) s[r][0] = row[wrap(c.x0 - 1, W)];
+    if (lane == 1) s[r][33] = row[wrap(c.x0 + kChunk, W)];
+  }
+  __syncwarp();
+}
+
+// The lane's channel pair of interior pixel (b, y, x) and its circular halo copies.
+__device__ __forceinline__ void put2(__nv_bfloat16* out, int H, int W, int b, int y, int x, int lane,
+                                     __nv_bfloat162 v) {
+  const int Hp = H + 2, Wp = W + 2;
+  const int y2 = (y == 0) ? H + 1 : (y == H - 1 ? 0 : -1);
+  const int x2 = (x == 0) ? W + 1 : (x == W - 1 ? 0 : -1);
+  reinterpret_cast<__nv_bfloat162*>(out + (((size_t)b * Hp + y + 1) * Wp + x + 1) * 64)[lane] = v;
+  if (y2 >= 0) reinterpret_cast<__nv_bfloat162*>(out + (((size_t)b * Hp + y2) * Wp + x + 1) * 64)[lane] = v;
+  if (x2 >= 0) {
+    reinterpret_cast<__nv_bfloat162*>(out + (((size_t)b * Hp + y + 1) * Wp + x2) * 64)[lane] = v;
+    if (y2 >= 0) reinterpret_cast<__nv_bfloat162*>(out + (((size_t)b * Hp + y2) * Wp + x2) * 64)[lane] = v;
   }
 }
 
-// Layer 1 forward: z = conv3x3(x; w[9][64]) + b (1 -> 64), a = gelu(z).
-__global__ void k_conv_in(int B, int H, int W, const float* __restrict__ x, const float* __restrict__ w,
-                          const float* __restrict__ bias, __nv_bfloat16* __restrict__ z,
-                          __nv_bfloat16* __restrict__ a_pad) {
-  const size_t n = (size_t)B * H * W;
-  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
-    const int xx = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((size_t)W * H));
-    float xv[9];
-#pragma unroll
-    for (int t = 0; t < 9; ++t) {
-      const int yy = wrap(y + t / 3 - 1, H), xw = wrap(xx + t % 3 - 1, W);
-      xv[t] = x[((size_t)b * H + yy) * W + xw];
-    }
-    float zf[64], af[64];
-#pragma unroll 8
-    for (int c = 0; c < 64; ++c) {
-      float s = bias[c];
-#pragma unroll
-      for (int t = 0; t < 9; ++t) s += xv[t] * w[t * 64 + c];
-      const float zb = __bfloat162float(__float2bfloat16_rn(s));
-      zf[c] = zb;
-      af[c] = gelu(zb);
-    }
-    uint4* zo = reinterpret_cast<uint4*>(z + p * 64);
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      uint4 v;
-      __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&v);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) h[j] = __floats2bfloat162_rn(zf[8 * i + 2 * j], zf[8 * i + 2 * j + 1]);
-      zo[i] = v;
-    }
-    put_halo(a_pad, H, W, b, y, xx, af);
-  }
+__device__ __forceinline__ float2 ld2(const __nv_bfloat16* t, size_t pix, int lane) {
+  return __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(t + pix * 64)[lane]);
 }
 
-// Last layer forward: y = conv3x3(a; w[9][64]) + b (64 -> 1), FP32 output.
-__global__ void k_conv_out(int B, int H, int W, const __nv_bfloat16* __restrict__ a_pad, const float* __restrict__ w,
-                           const float* __restrict__ bias, float* __restrict__ y) {
-  __shared__ float sw[9 * 64];
-  for (int i = threadIdx.x; i < 9 * 64; i += blockDim.x) sw[i] = w[i];
-  __syncthreads();
-  const size_t n = (size_t)B * H * W;
-  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
-    const int xx = (int)(p % W), yy = (int)((p / W) % H), b = (int)(p / ((size_t)W * H));
-    float s = bias[0];
-    for (int t = 0; t < 9; ++t) {
-      const uint4* src = reinterpret_cast<const uint4*>(a_pad + padidx(b, yy + t / 3 - 1, xx + t % 3 - 1, H, W) * 64);
+// After the call lane l holds, in v[0], the sum over all lanes of their v[l].
+__device__ __forceinline__ float reduce_scatter32(float (&v)[32], int lane) {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const uint4 v = src[i];
-        const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&v);
+  for (int off = 16; off >= 1; off >>= 1) {
+    const bool upper = (lane & off) != 0;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const float2 f = __bfloat1622float2(h[j]);
-          s += f.x * sw[t * 64 + 8 * i + 2 * j] + f.y * sw[t * 64 + 8 * i + 2 * j + 1];
-        }
+    for (int i = 0; i < off; ++i) {
+      const float send = upper ? v[i] : v[i + off];
+      const float keep = upper ? v[i + off] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+    }
+  }
+  return v[0];
+}
+
+// Layer 1 forward: z = conv3x3(in_scale x; w[9][64]) + b (1 -> 64), a = gelu(z).
+__global__ void __launch_bounds__(kWarps * 32) k_conv_in(int B, int H, int W, float in_scale, const float* __restrict__ x,
+                                                         const float* __restrict__ w, const float* __restrict__ bias,
+                                                         __nv_bfloat16* __restrict__ z, __nv_bfloat16* __restrict__ a_pad) {
+  __shared__ float stg[kWarps][3][34];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float w0[9], w1[9];
+#pragma unroll
+  for (int t = 0; t < 9; ++t) {
+    w0[t] = w[t * 64 + 2 * lane] * in_scale;
+    w1[t] = w[t * 64 + 2 * lane + 1] * in_scale;
+  }
+  const float b0 = bias[2 * lane], b1 = bias[2 * lane + 1];
+  const size_t n_chunks = (size_t)B * H * W / kChunk;
+  for (size_t ch = (size_t)blockIdx.x * kWarps + warp; ch < n_chunks; ch += (size_t)gridDim.x * kWarps) {
+    const Chunk c = chunk_of(ch, H, W);
+    __syncwarp();
+    stage_rows(stg[warp], x, H, W, c, lane);
+    for (int j = 0; j < kChunk; ++j) {
+      float s0 = b0, s1 = b1;
+#pragma unroll
+      for (int t = 0; t < 9; ++t) {
+        const float xv = stg[warp][t / 3][j + t % 3];
+        s0 += xv * w0[t];
+        s1 += xv * w1[t];
       }
+      const __nv_bfloat162 zb = __floats2bfloat162_rn(s0, s1);
+      reinterpret_cast<__nv_bfloat162*>(z + (c.p0 + j) * 64)[lane] = zb;
+      const float2 zf = __bfloat1622float2(zb);
+      put2(a_pad, H, W, c.b, c.y, c.x0 + j, lane, __floats2bfloat162_rn(gelu(zf.x), gelu(zf.y)));
     }
-    y[p] = s;
+  }
+}
+
+// Last layer forward: y = out_scale (conv3x3(a; w[9][64]) + b) (64 -> 1), FP32.
+__global__ void __launch_bounds__(kWarps * 32) k_conv_out(int B, int H, int W, float out_scale,
+                                                          const __nv_bfloat16* __restrict__ a_pad,
+                                                          const float* __restrict__ w, const float* __restrict__ bias,
+                                                          float* __restrict__ y) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float w0[9], w1[9];
+#pragma unroll
+  for (int t = 0; t < 9; ++t) {
+    w0[t] = w[t * 64 + 2 * lane];
+    w1[t] = w[t * 64 + 2 * lane + 1];
+  }
+  const float bb = bias[0];
+  const size_t n_chunks = (size_t)B * H * W / kChunk;
+  for (size_t ch = (size_t)blockIdx.x * kWarps + warp; ch < n_chunks; ch += (size_t)gridDim.x * kWarps) {
+    const Chunk c = chunk_of(ch, H, W);
+    float acc[kChunk];
+#pragma unroll
+    for (int j = 0; j < kChunk; ++j) {
+      float s = 0.f;
+#pragma unroll
+      for (int t = 0; t < 9; ++t) {
+        const float2 f = ld2(a_pad, padidx(c.b, c.y + t / 3 - 1, c.x0 + j + t % 3 - 1, H, W), lane);
+        s += f.x * w0[t] + f.y * w1[t];
+      }
+      acc[j] = s;
+    }
+    const float tot = reduce_scatter32(acc, lane);
+    y[c.p0 + lane] = (tot + bb) * out_scale;
   }
 }
 
 // Last layer backward, data part: g_a[q][c] = sum_t gy[q - off_t] w[t][c],
-// then times gelu'(z[q][c]) -> halo'd BF16 gradient of the layer-5 pre-activation.
-__global__ void k_conv_out_dgrad(int B, int H, int W, const float* __restrict__ gy, const float* __restrict__ w,
-                                 const __nv_bfloat16* __restrict__ z, __nv_bfloat16* __restrict__ gz_pad) {
-  __shared__ float sw[9 * 64];
-  for (int i = threadIdx.x; i < 9 * 64; i += blockDim.x) sw[i] = w[i];
-  __syncthreads();
-  const size_t n = (size_t)B * H * W;
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-    const int xx = (int)(q % W), yy = (int)((q / W) % H), b = (int)(q / ((size_t)W * H));
-    float g9[9];
+// times gelu'(z[q][c]) -> halo'd BF16 gradient of the layer-5 pre-activation.
+__global__ void __launch_bounds__(kWarps * 32) k_conv_out_dgrad(int B, int H, int W, const float* __restrict__ gy,
+                                                                const float* __restrict__ w,
+                                                                const __nv_bfloat16* __restrict__ z,
+                                                                __nv_bfloat16* __restrict__ gz_pad) {
+  __shared__ float stg[kWarps][3][34];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float w0[9], w1[9];
 #pragma unroll
-    for (int t = 0; t < 9; ++t) {
-      const int py = wrap(yy - (t / 3 - 1), H), px = wrap(xx - (t % 3 - 1), W);
-      g9[t] = gy[((size_t)b * H + py) * W + px];
-    }
-    const uint4* zs = reinterpret_cast<const uint4*>(z + q * 64);
-    float out[64];
+  for (int t = 0; t < 9; ++t) {
+    w0[t] = w[t * 64 + 2 * lane];
+    w1[t] = w[t * 64 + 2 * lane + 1];
+  }
+  const size_t n_chunks = (size_t)B * H * W / kChunk;
+  for (size_t ch = (size_t)blockIdx.x * kWarps + warp; ch < n_chunks; ch += (size_t)gridDim.x * kWarps) {
+    const Chunk c = chunk_of(ch, H, W);
+    __syncwarp();
+    stage_rows(stg[warp], gy, H, W, c, lane);
+    for (int j = 0; j < kChunk; ++j) {
+      float s0 = 0.f, s1 = 0.f;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const uint4 v = zs[i];
-      const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&v);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const float2 zz = __bfloat1622float2(h[j]);
-        const int c = 8 * i + 2 * j;
-        float s0 = 0.f, s1 = 0.f;
-#pragma unroll
-        for (int t = 0; t < 9; ++t) {
-          s0 += g9[t] * sw[t * 64 + c];
-          s1 += g9[t] * sw[t * 64 + c + 1];
-        }
-        out[c] = s0 * gelu_grad(zz.x);
-        out[c + 1] = s1 * gelu_grad(zz.y);
+      for (int t = 0; t < 9; ++t) {  // gy at (y - dy, x - dx)
+        const float g = stg[warp][2 - t / 3][j + 2 - t % 3];
+        s0 += g * w0[t];
+        s1 += g * w1[t];
       }
+      const float2 zz = ld2(z, c.p0 + j, lane);
+      put2(gz_pad, H, W, c.b, c.y, c.x0 + j, lane, __floats2bfloat162_rn(s0 * gelu_grad(zz.x), s1 * gelu_grad(zz.y)));
     }
-    put_halo(gz_pad, H, W, b, yy, xx, out);
   }
 }
 
-// Per-block partial sums of the small-layer gradients (fixed grid).
+// Per-block partial sums of the small-layer gradients (fixed grid, fixed order).
 //  mode 0 (last layer):  part[blk][t*64 + c] = sum_p gy[p] a[p + t][c]; part[blk][576] = sum gy
 //  mode 1 (first layer): part[blk][t*64 + c] = sum_p gz[p][c] x[p + t];  part[blk][576 + c] = sum gz[.][c]
-//  mode 2 (bias of a middle layer): part[blk][c] = sum_p gz[p][c]
+//  mode 2 (bias of a middle layer): part[blk][576 + c] = sum_p gz[p][c]
 constexpr int kRedBlocks = 296;
 constexpr int kRedStride = 9 * 64 + 64;
-__global__ void k_small_grad_partial(int mode, int B, int H, int W, const float* __restrict__ gy,
-                                     const __nv_bfloat16* __restrict__ a_pad, const float* __restrict__ x,
-                                     const __nv_bfloat16* __restrict__ gz_pad, float* __restrict__ part) {
+__global__ void __launch_bounds__(kWarps * 32) k_small_grad_partial(int mode, int B, int H, int W,
+                                                                    const float* __restrict__ gy,
+                                                                    const __nv_bfloat16* __restrict__ a_pad,
+                                                                    const float* __restrict__ x,
+                                                                    const __nv_bfloat16* __restrict__ gz_pad,
+                                                                    float* __restrict__ part) {
   __shared__ float acc[kRedStride];
+  __shared__ float stg[kWarps][3][34];
   for (int i = threadIdx.x; i < kRedStride; i += blockDim.x) acc[i] = 0.f;
   __syncthreads();
-  const size_t n = (size_t)B * H * W;
-  // each thread keeps its own channel slice: thread (c = threadIdx.x % 64) accumulates channel c
-  const int c = threadIdx.x & 63, lanes = blockDim.x / 64, sub = threadIdx.x / 64;
-  float loc[10];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float a0[9], a1[9];
 #pragma unroll
-  for (int i = 0; i < 10; ++i) loc[i] = 0.f;
-  for (size_t p = blockIdx.x * (size_t)lanes + sub; p < n; p += (size_t)gridDim.x * lanes) {
-    const int xx = (int)(p % W), yy = (int)((p / W) % H), b = (int)(p / ((size_t)W * H));
+  for (int t = 0; t < 9; ++t) a0[t] = a1[t] = 0.f;
+  float s0 = 0.f, s1 = 0.f;
+  const size_t n_chunks = (size_t)B * H * W / kChunk;
+  for (size_t ch = (size_t)blockIdx.x * kWarps + warp; ch < n_chunks; ch += (size_t)gridDim.x * kWarps) {
+    const Chunk c = chunk_of(ch, H, W);
     if (mode == 0) {
-      const float g = gy[p];
+      const float gv = gy[c.p0 + lane];
+      s0 += gv;
+      for (int j = 0; j < kChunk; ++j) {
+        const float g = __shfl_sync(0xffffffffu, gv, j);
 #pragma unroll
-      for (int t = 0; t < 9; ++t)
-        loc[t] += g * __bfloat162float(a_pad[padidx(b, yy + t / 3 - 1, xx + t % 3 - 1, H, W) * 64 + c]);
-      if (c == 0) loc[9] += g;
+        for (int t = 0; t < 9; ++t) {
+          const float2 f = ld2(a_pad, padidx(c.b, c.y + t / 3 - 1, c.x0 + j + t % 3 - 1, H, W), lane);
+          a0[t] += g * f.x;
+          a1[t] += g * f.y;
+        }
+      }
     } else if (mode == 1) {
-      const float g = __bfloat162float(gz_pad[padidx(b, yy, xx, H, W) * 64 + c]);
+      __syncwarp();
+      stage_rows(stg[warp], x, H, W, c, lane);
+      for (int j = 0; j < kChunk; ++j) {
+        const float2 g = ld2(gz_pad, padidx(c.b, c.y, c.x0 + j, H, W), lane);
 #pragma unroll
-      for (int t = 0; t < 9; ++t) loc[t] += g * x[((size_t)b * H + wrap(yy + t / 3 - 1, H)) * W + wrap(xx + t % 3 - 1, W)];
-      loc[9] += g;
+        for (int t = 0; t < 9; ++t) {
+          const float xv = stg[warp][t / 3][j + t % 3];
+          a0[t] += g.x * xv;
+          a1[t] += g.y * xv;
+        }
+        s0 += g.x;
+        s1 += g.y;
+      }
     } else {
-      loc[9] += __bfloat162float(gz_pad[padidx(b, yy, xx, H, W) * 64 + c]);
+      for (int j = 0; j < kChunk; ++j) {
+        const float2 g = ld2(gz_pad, padidx(c.b, c.y, c.x0 + j, H, W), lane);
+        s0 += g.x;
+        s1 += g.y;
+      }
     }
   }
-  // fixed-order combination of the block's threads
-  for (int s = 0; s < lanes; ++s) {
-    if (sub == s) {
-      for (int t = 0; t < 9; ++t) acc[t * 64 + c] += loc[t];
-      acc[576 + c] += loc[9];
+  if (mode == 0) {  // sum of gy over the warp's pixels (fixed order)
+    for (int o = 16; o >= 1; o >>= 1) s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+  }
+  // fixed-order combination of the block's warps
+  for (int wv = 0; wv < kWarps; ++wv) {
+    if (warp == wv) {
+      if (mode != 2) {
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+          acc[t * 64 + 2 * lane] += a0[t];
+          acc[t * 64 + 2 * lane + 1] += a1[t];
+        }
+      }
+      if (mode == 0) {
+        if (lane == 0) acc[576] += s0;
+      } else {
+        acc[576 + 2 * lane] += s0;
+        acc[576 + 2 * lane + 1] += s1;
+      }
     }
     __syncthreads();
   }
@@ -254,39 +332,56 @@ __global__ void k_weights_bf16(const float* __restrict__ w, __nv_bfloat16* __res
   wb[((size_t)(8 - t) * 64 + ci) * 64 + co] = h;
 }
 
-// FP32 [B][H][W] -> halo'd scalar copy is not needed: layers read x with wrap.
+bool shape_ok(int B, int H, int W) { return B >= 1 && H >= 2 && W >= kChunk && W % kChunk == 0; }
+
+// Chunked kernels: enough blocks for every SM several times over, no more
+// blocks than there are chunks to share.
+int grid_for(int B, int H, int W) {
+  const size_t blocks = ((size_t)B * H * W / kChunk + kWarps - 1) / kWarps;
+  return (int)(blocks < 1184 ? blocks : 1184);
+}
 
 }  // namespace
 
 extern "C" {
 
-int closure_conv_in(int32_t B, int32_t H, int32_t W, const float* x, const float* w, const float* bias, void* z,
-                    void* a_pad, void* stream) {
+int closure_conv_in(int32_t B, int32_t H, int32_t W, float in_scale, const float* x, const float* w, const float* bias,
+                    void* z, void* a_pad, void* stream) {
   if (!x || !w || !bias || !z || !a_pad) return ofail("closure_conv_in: null pointer");
-  k_conv_in<<<592, 128, 0, (cudaStream_t)stream>>>(B, H, W, x, w, bias, (__nv_bfloat16*)z, (__nv_bfloat16*)a_pad);
+  if (!shape_ok(B, H, W)) return ofail("closure_conv_in: need B >= 1, H >= 2 and W a positive multiple of 32");
+  k_conv_in<<<grid_for(B, H, W), kWarps * 32, 0, (cudaStream_t)stream>>>(B, H, W, in_scale, x, w, bias,
+                                                                         (__nv_bfloat16*)z, (__nv_bfloat16*)a_pad);
   return cudaGetLastError() == cudaSuccess ? 0 : ofail("closure_conv_in: launch failed");
 }
 
-int closure_conv_out(int32_t B, int32_t H, int32_t W, const void* a_pad, const float* w, const float* bias, float* y,
-                     void* stream) {
+int closure_conv_out(int32_t B, int32_t H, int32_t W, float out_scale, const void* a_pad, const float* w,
+                     const float* bias, float* y, void* stream) {
   if (!a_pad || !w || !bias || !y) return ofail("closure_conv_out: null pointer");
-  k_conv_out<<<592, 128, 0, (cudaStream_t)stream>>>(B, H, W, (const __nv_bfloat16*)a_pad, w, bias, y);
+  if (!shape_ok(B, H, W)) return ofail("closure_conv_out: need B >= 1, H >= 2 and W a positive multiple of 32");
+  k_conv_out<<<grid_for(B, H, W), kWarps * 32, 0, (cudaStream_t)stream>>>(B, H, W, out_scale,
+                                                                          (const __nv_bfloat16*)a_pad, w, bias, y);
   return cudaGetLastError() == cudaSuccess ? 0 : ofail("closure_conv_out: launch failed");
 }
 
 int closure_conv_out_dgrad(int32_t B, int32_t H, int32_t W, const float* gy, const float* w, const void* z,
                            void* gz_pad, void* stream) {
   if (!gy || !w || !z || !gz_pad) return ofail("closure_conv_out_dgrad: null pointer");
-  k_conv_out_dgrad<<<592, 128, 0, (cudaStream_t)stream>>>(B, H, W, gy, w, (const __nv_bfloat16*)z,
-                                                          (__nv_bfloat16*)gz_pad);
+  if (!shape_ok(B, H, W)) return ofail("closure_conv_out_dgrad: need B >= 1, H >= 2 and W a positive multiple of 32");
+  k_conv_out_dgrad<<<grid_for(B, H, W), kWarps * 32, 0, (cudaStream_t)stream>>>(B, H, W, gy, w,
+                                                                                (const __nv_bfloat16*)z,
+                                                                                (__nv_bfloat16*)gz_pad);
   return cudaGetLastError() == cudaSuccess ? 0 : ofail("closure_conv_out_dgrad: launch failed");
 }
 
 int closure_small_grad(int32_t mode, int32_t B, int32_t H, int32_t W, const float* gy, const void* a_pad,
                        const float* x, const void* gz_pad, float* partials, float* out, void* stream) {
   if (!partials || !out) return ofail("closure_small_grad: null pointer");
+  if (!shape_ok(B, H, W)) return ofail("closure_small_grad: need B >= 1, H >= 2 and W a positive multiple of 32");
+  if (mode < 0 || mode > 2) return ofail("closure_small_grad: mode must be 0, 1 or 2");
+  if ((mode == 0 && (!gy || !a_pad)) || (mode == 1 && (!x || !gz_pad)) || (mode == 2 && !gz_pad))
+    return ofail("closure_small_grad: null input");
   cudaStream_t st = (cudaStream_t)stream;
-  k_small_grad_partial<<<kRedBlocks, 256, 0, st>>>(mode, B, H, W, gy, (const __nv_bfloat16*)a_pad, x,
+  k_small_grad_partial<<<kRedBlocks, kWarps * 32, 0, st>>>(mode, B, H, W, gy, (const __nv_bfloat16*)a_pad, x,
                                                    (const __nv_bfloat16*)gz_pad, partials);
   k_small_grad_final<<<3, 256, 0, st>>>(kRedBlocks, partials, out);
   return cudaGetLastError() == cudaSuccess ? 0 : ofail("closure_small_grad: launch failed");
