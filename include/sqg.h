@@ -144,6 +144,15 @@ int sqg_stage_begin(sqg_plan* plan, const void* theta_in, void* stream);
 int sqg_stage(sqg_plan* plan, int32_t stage, const void* theta_in, void* theta_out,
               double dt, const void* extra_rhs, const double* ring_phases, void* stream);
 
+/* The same stage with an extra tendency given in physical space: src is a
+ * real N x N field of the plan precision, and the stage right-hand side is
+ * -mask fft2(u.grad theta - src) + (linear terms, forcing): src is added to
+ * the advective term inside the column pass and dealiased with it (a learned
+ * subgrid closure enters the coarse solve this way).  Extension: the
+ * reference adds forcing terms in spectral space only (solver.py:170-178). */
+int sqg_stage_physical(sqg_plan* plan, int32_t stage, const void* theta_in, void* theta_out,
+                       double dt, const void* src, const double* ring_phases, void* stream);
+
 /* Velocity (u, v) in physical space (replaces compute_velocity_from_theta,
  * operators.py:159-181).  u and v: N x N real of the plan precision. */
 int sqg_velocity(sqg_plan* plan, const void* theta_hat, void* u, void* v, void* stream);

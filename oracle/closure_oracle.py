@@ -2,22 +2,27 @@
 
 No reference counterpart: the reference has no learned closure.  Six 3x3
 convolutions with circular padding (1 -> 64 -> 64 -> 64 -> 64 -> 64 -> 1),
-exact GELU between them; forward and analytic backward.  Parameter layout
+GELU (tanh form) between them; forward and analytic backward.  Parameter layout
 matches pygsquig_b200.closure.cnn: w1 [9, 64], wl [9, 64 out, 64 in],
 w6 [9, 64], tap t = 3 (dy + 1) + (dx + 1), out[p] = sum_t in[p + off_t].
 The analytic gradients are checked against finite differences in the tests.
 """
 
 import numpy as np
-from scipy.special import erf
+
+
+GELU_A = np.sqrt(2.0 / np.pi)
+GELU_B = 0.044715
 
 
 def gelu(z):
-    return 0.5 * z * (1 + erf(z / np.sqrt(2)))
+    """GELU in its tanh form (Hendrycks & Gimpel 2016), the network's activation."""
+    return 0.5 * z * (1 + np.tanh(GELU_A * (z + GELU_B * z**3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1 + erf(z / np.sqrt(2))) + z * np.exp(-0.5 * z * z) / np.sqrt(2 * np.pi)
+    t = np.tanh(GELU_A * (z + GELU_B * z**3))
+    return 0.5 * (1 + t) + 0.5 * z * (1 - t * t) * GELU_A * (1 + 3 * GELU_B * z * z)
 
 
 def shift(x, t):

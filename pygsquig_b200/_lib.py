@@ -80,6 +80,7 @@ SIGNATURES = {
     "sqg_multistep": [_vp, _vp, _i32, _dbl, _vp, _i32, _vp],
     "sqg_stage_begin": [_vp, _vp, _vp],
     "sqg_stage": [_vp, _i32, _vp, _vp, _dbl, _vp, _vp, _vp],
+    "sqg_stage_physical": [_vp, _i32, _vp, _vp, _dbl, _vp, _vp, _vp],
     "sqg_velocity": [_vp, _vp, _vp, _vp, _vp],
     "sqg_to_physical": [_vp, _vp, _vp, _vp],
     "sqg_to_spectral": [_vp, _vp, _vp, _vp],

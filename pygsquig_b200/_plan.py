@@ -186,6 +186,12 @@ class Plan:
         _lib.check(self._lib.sqg_stage(self._h, int(s), th_in.data_ptr(), th_out.data_ptr(), float(dt), _ptr(extra),
                                        _ptr(phases), _stream_ptr()))
 
+    def stage_physical(self, s, th_in, th_out, dt, src, phases=None):
+        """Stage s with a physical-space tendency ``src`` (real N x N, plan
+        precision) added to the advective term and dealiased with it."""
+        _lib.check(self._lib.sqg_stage_physical(self._h, int(s), th_in.data_ptr(), th_out.data_ptr(), float(dt),
+                                                src.data_ptr(), _ptr(phases), _stream_ptr()))
+
     def velocity(self, th):
         N = self.key.N
         u = torch.empty((N, N), dtype=self.rdtype, device=self.device)

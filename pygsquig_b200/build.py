@@ -1,6 +1,12 @@
 """Build libsqg.so in-tree with nvcc for sm_100a.
 
     python -m pygsquig_b200.build [--force]
+
+Each translation unit is compiled to an object under ``_build/`` (rebuilt
+when it or a header it includes changed) and the objects are linked into
+``libsqg.so`` beside this file.  The library counts as up to date when it is
+newer than every source and header, so a copy that carries the library but
+not the objects does not rebuild.
 """
 
 from __future__ import annotations
@@ -11,13 +17,19 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRCS = [os.path.join(HERE, "csrc", f) for f in ("sqg_capi.cu", "closure_conv.cu", "closure_ops.cu")]
-DEPS = [os.path.join(HERE, "csrc", f) for f in ("sqg_fft.cuh", "sqg_kernels.cuh", "sqg_aux.cuh")] + [
-    os.path.join(ROOT, "include", f) for f in ("sqg.h", "sqg_closure.h")]
+CSRC = os.path.join(HERE, "csrc")
+SRCS = [os.path.join(CSRC, f) for f in ("sqg_capi.cu", "closure_conv.cu", "closure_ops.cu")]
+# headers each unit includes (a change rebuilds the unit)
+DEPS = {
+    "sqg_capi.cu": ["sqg_fft.cuh", "sqg_kernels.cuh", "sqg_aux.cuh", "../../include/sqg.h"],
+    "closure_conv.cu": ["closure_act.cuh", "../../include/sqg_closure.h"],
+    "closure_ops.cu": ["closure_act.cuh", "../../include/sqg_closure.h"],
+}
 OUT = os.path.join(HERE, "libsqg.so")
+OBJ_DIR = os.path.join(HERE, "_build")
 
-NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
-              "-Xcompiler", "-fPIC", "-shared"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-std=c++17"] + ARCH + ["-lineinfo", "-Xcompiler", "-fPIC"]
 
 
 def nvcc() -> str:
@@ -27,17 +39,41 @@ def nvcc() -> str:
     return "nvcc"
 
 
+def _obj(src: str) -> str:
+    return os.path.join(OBJ_DIR, os.path.basename(src)[:-3] + ".o")
+
+
+def _deps(src: str):
+    return [src] + [os.path.normpath(os.path.join(CSRC, d)) for d in DEPS[os.path.basename(src)]]
+
+
+def _stale(target: str, inputs) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(p) > t for p in inputs)
+
+
 def up_to_date() -> bool:
-    if not os.path.exists(OUT):
-        return False
-    t = os.path.getmtime(OUT)
-    return all(os.path.getmtime(p) <= t for p in SRCS + DEPS)
+    """The library exists and is newer than every source and header."""
+    return not _stale(OUT, [p for s in SRCS for p in _deps(s)])
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return OUT
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", OUT + ".tmp"] + SRCS
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    objs = []
+    for s in SRCS:
+        o = _obj(s)
+        if force or _stale(o, _deps(s)):
+            cmd = [nvcc()] + NVCC_FLAGS + ["-c", "-o", o + ".tmp", s]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.run(cmd, check=True)
+            os.replace(o + ".tmp", o)
+        objs.append(o)
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", OUT + ".tmp"] + objs
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -5,9 +5,14 @@ The closure models the nonlinear term the coarse grid cannot carry,
     Pi = filter(-mask fft2(u.grad theta)) - (-mask_c fft2(u_c.grad theta_c)),
 with theta_c = filter(theta) (the sharp filter of spectral.SpectralFilter).
 It is evaluated on every RK stage input: theta_s -> physical theta (library
-transform) -> CNN (library kernels, BF16 tensor cores) -> spectrum (library
-transform) -> restricted to the coarse dealiased disk and added to that
-stage's right-hand side, exactly where the solver adds any forcing term.
+transform) -> CNN (library kernels, BF16 tensor cores) -> Pi(x, y).  As a
+generic forcing term (``SubgridClosure.__call__``) Pi is transformed,
+restricted to the coarse dealiased disk and added to that stage's
+right-hand side, exactly where the solver adds any forcing term; the coarse
+solver below instead hands Pi(x, y) to the stage kernels
+(sqg_stage_physical), which subtract it from u.grad(theta) before the
+forward transform and dealias the sum -- the same term without a separate
+transform.
 """
 
 from __future__ import annotations
@@ -59,6 +64,15 @@ class SubgridClosure:
             self.x[0].copy_(self.phys)
         return self.net.forward(self.x, in_scale=1.0 / self.sigma_theta,
                                 out_scale=1.0 if normalised else self.sigma_pi)[0]
+
+    def source(self, theta_hat: torch.Tensor) -> torch.Tensor:
+        """Pi in physical space in the plan precision (the form the solver's
+        stage kernels add to the advective term, sqg_stage_physical)."""
+        y = self.physical(theta_hat)
+        if self.yspec_in.dtype != y.dtype:
+            self.yspec_in.copy_(y)
+            return self.yspec_in
+        return y
 
     def __call__(self, theta_hat: torch.Tensor, **kwargs) -> torch.Tensor:
         y = self.physical(theta_hat)
@@ -113,8 +127,10 @@ class ClosureSolver:
         pl.stage_begin(self.th_a)
         for s in range(1, 5):
             th_s = self.th_a if s == 1 else stage_buf
-            extra = self.closure(th_s) if self.closure is not None else None
-            pl.stage(s, self.th_a, self.th_b, dt, extra, ph)
+            if self.closure is not None:
+                pl.stage_physical(s, self.th_a, self.th_b, dt, self.closure.source(th_s), ph)
+            else:
+                pl.stage(s, self.th_a, self.th_b, dt, None, ph)
         self.th_a.copy_(self.th_b)
 
     def _capture(self, dt):

@@ -4,27 +4,36 @@
 // Implicit GEMM: M = 128 pixels of one image row (a tile), N = 64 output
 // channels, K = 9 taps x 64 input channels (one 64-wide K block per tap).
 // Activations are NHWC BF16 with a one-pixel circular halo.  For each of the
-// three input rows a tile needs, one TMA box brings 130 pixels (the tile and
-// its two neighbours) into shared memory in the unswizzled K-major core-matrix
-// layout (8 pixels x 16 bytes per core matrix, channel groups 130 x 16 bytes
-// apart), so the A operand of tap (dy, dx) is the slab of row dy read from
-// pixel dx: a 16-byte shift of the descriptor start.  Each activation byte is
-// fetched three times instead of nine.  The weights of the 9 taps stay in
-// shared memory (128B-swizzled, K-major) for the life of the persistent CTA.
+// three input rows a tile needs, one TMA box brings 130 consecutive pixels
+// (the tile and its two neighbours: 130 rows of 128 bytes, 128B-swizzled)
+// into a 1024-byte aligned slab.  The A operand of tap (dy, dx) is the slab of
+// row dy read from row dx: the descriptor start moves by dx rows (base offset
+// 0: the 128-byte swizzle follows the absolute shared-memory address bits,
+// as the TMA wrote them, so a row-shifted start reads the same layout).  Each
+// activation byte is fetched three times instead of nine, in 128-byte rows.
+// The weights of the 9 taps stay in shared memory (128B-swizzled, K-major)
+// for the life of the persistent CTA.
 //
 // Warp roles (10 warps): warp 0 issues TMA loads, warp 1 allocates TMEM and
 // issues the MMAs (one elected thread), warps 2..9 read the FP32 accumulators
 // from TMEM (tcgen05.ld; warp w may read lane quarter w % 4, so two warps
 // share each quarter and take 32 of the 64 columns each) and run the
-// epilogue.  Two
-// TMEM accumulators alternate so the epilogue of tile i overlaps the MMAs of
-// tile i+1.  Every mbarrier wait is bounded: on time-out the kernel records
-// an error flag and the roles drain and return.
+// epilogue.  A tile accumulates into four TMEM accumulators, one per 16-wide
+// slice of the 64 input channels, so consecutive MMAs never wait on each
+// other's result (a single 128 x 64 accumulator chain of 36 short MMAs is
+// latency-bound); the epilogue adds the four.  Two such sets alternate so the
+// epilogue of tile i overlaps the MMAs of tile i+1 (512 TMEM columns).  The epilogue writes its BF16 outputs into
+// 128B-swizzled staging tiles, and one thread stores each tile (and its copy
+// on the halo row when the image row is the first or last) with a TMA tensor
+// store; the halo-column copies of the first and last pixel of an image row
+// are plain stores.  Every mbarrier wait is bounded: on time-out the kernel
+// records an error flag, the epilogue warps agree through a barrier
+// reduction, and all roles drain and return.
 //
 // Epilogues:
 //   FWD:   z = acc + bias; store z (BF16, unpadded) and gelu(z) (BF16, halo'd)
 //   DGRAD: g = acc * gelu'(zprev); store g (BF16, halo'd)
-//   LIN:   store acc + bias (FP32, unpadded)
+//   LIN:   store acc + bias (FP32, unpadded; plain stores)
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -34,6 +43,7 @@
 #include <string>
 
 #include "../../include/sqg_closure.h"
+#include "closure_act.cuh"
 
 namespace {
 
@@ -43,15 +53,14 @@ int cfail(int code, const std::string& m) {
   return code;
 }
 
-constexpr int kStages = 6;
 constexpr int kTileM = 128;
 constexpr int kC = 64;
-constexpr int kSlabPix = kTileM + 2;       // pixels of one input-row slab
-constexpr int kSlabBytes = kSlabPix * kC * 2;  // 16640 B
-// Guard band after the slabs: every descriptor address stays inside the
-// allocation even if a stride were misread.
-constexpr int kSmemGuard = 32768;
-constexpr int kBBytes = kC * kC * 2;      // 8 KB per tap
+constexpr int kSlabRows = kTileM + 2;        // pixels of one input-row slab
+constexpr int kSlabBytes = kSlabRows * 128;  // 16640 B loaded per slab
+constexpr int kSlabStride = 17 * 1024;       // slabs start on 1024-byte boundaries
+constexpr int kStages = 6;                   // slabs in flight (two tiles)
+constexpr int kBBytes = kC * kC * 2;         // 8 KB per tap
+constexpr int kStageTile = kTileM * 128;     // 16 KB staging tile (128 pixels x 64 BF16)
 constexpr int kThreads = 320;
 constexpr int kEpiWarps = 8;
 constexpr uint32_t kWaitLimit = 1u << 26;
@@ -91,25 +100,45 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
       : "memory");
 }
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void* src, int x, int y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];\n" ::"l"(map),
+               "r"(smem_u32(src)), "r"(x), "r"(y)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+// the staging tiles may be rewritten once the stores issued so far have read them
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+// generic-proxy shared-memory writes become visible to the TMA (async proxy)
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// named barrier 1 over the 8 epilogue warps
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 256;\n" ::: "memory"); }
+// the same barrier with an OR over the epilogue threads' predicates
+__device__ __forceinline__ int epi_sync_or(int pred) {
+  int r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.s32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, 256, p;\n\t"
+      "selp.s32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"(pred)
+      : "memory");
+  return r;
+}
 __device__ __forceinline__ uint64_t sw128_desc(const void* smem_tile) {
   // K-major, 128-byte swizzle: rows of 128 B, 8-row groups 1024 B apart
   const uint64_t start = (smem_u32(smem_tile) >> 4) & 0x3FFF;
   const uint64_t lbo = 1, sbo = 1024 >> 4;
   return start | (lbo << 16) | (sbo << 32) | (1ull << 46) | (2ull << 61);
 }
-// K-major, no swizzle: core matrices of 8 pixels x 16 B (128 B contiguous),
-// next 8 pixels 128 B away (SBO), next 8 channels one slab row-group away (LBO)
-__device__ __forceinline__ uint64_t slab_desc(const void* slab) {
-  const uint64_t start = (smem_u32(slab) >> 4) & 0x3FFF;
-  const uint64_t lbo = (kSlabPix * 16) >> 4, sbo = 128 >> 4;
-  return start | (lbo << 16) | (sbo << 32) | (1ull << 46);
-}
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];\n" ::"r"(
-          smem_u32(dst)),
-      "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
-      : "memory");
+// The same layout read from row `row` of a 1024-byte aligned slab: the start
+// moves by row x 128 B; the swizzle phase comes from the address bits.
+__device__ __forceinline__ uint64_t slab_desc(const void* slab, int row) {
+  const uint32_t addr = smem_u32(slab) + (uint32_t)row * 128u;
+  const uint64_t start = (addr >> 4) & 0x3FFF;
+  const uint64_t lbo = 1, sbo = 1024 >> 4;
+  return start | (lbo << 16) | (sbo << 32) | (1ull << 46) | (2ull << 61);
 }
 // BF16 x BF16 -> FP32, K-major A and B, M = 128, N = 64
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
@@ -139,51 +168,46 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
         "=r"(r[30]), "=r"(r[31])                                                                              \
       : "r"(addr))
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
-__device__ __forceinline__ float gelu_grad(float z) {
-  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
-}
-
 struct ConvArgs {
   int B, H, W;            // images, rows, columns (W multiple of 128)
   int mode;               // CLOSURE_EPI_*
   const float* bias;      // [64] (FWD, LIN)
   const __nv_bfloat16* zprev;  // [B][H][W][64] pre-activation of the layer below (DGRAD)
   __nv_bfloat16* out_pad;      // [B][H+2][W+2][64] halo'd output (FWD: gelu(z), DGRAD: g)
-  __nv_bfloat16* out_z;        // [B][H][W][64] pre-activation (FWD)
   float* out_f32;              // [B][H][W][64] (LIN)
   unsigned* err;
 };
 
-// Writes 32 BF16 channels (from channel c0) of pixel (b, y, x) to the halo'd
-// tensor, including their circular copies on the halo.
-__device__ __forceinline__ void store_halo(__nv_bfloat16* out, int H, int W, int b, int y, int x, int c0,
-                                           const uint4 (&v)[4]) {
+// Halo-column copies of 32 BF16 channels (from c0) of pixel (b, y, x), x the
+// first or last column: padded column W+1 or 0 of its row, and the corner
+// when y is also the first or last row.
+__device__ __forceinline__ void store_xhalo(__nv_bfloat16* out, int H, int W, int b, int y, int x, int c0,
+                                            const uint4 (&v)[4]) {
   const int Wp = W + 2, Hp = H + 2;
-  int ys[2] = {y + 1, -1}, xs[2] = {x + 1, -1};
-  if (y == 0) ys[1] = H + 1;
-  if (y == H - 1) ys[1] = 0;
-  if (x == 0) xs[1] = W + 1;
-  if (x == W - 1) xs[1] = 0;
+  const int xs = (x == 0) ? W + 1 : 0;
+  const int ys[2] = {y + 1, (y == 0) ? H + 1 : (y == H - 1 ? 0 : -1)};
   for (int a = 0; a < 2; ++a) {
     if (ys[a] < 0) continue;
-    for (int c = 0; c < 2; ++c) {
-      if (xs[c] < 0) continue;
-      uint4* dst = reinterpret_cast<uint4*>(out + (((size_t)b * Hp + ys[a]) * Wp + xs[c]) * kC + c0);
+    uint4* dst = reinterpret_cast<uint4*>(out + (((size_t)b * Hp + ys[a]) * Wp + xs) * kC + c0);
 #pragma unroll
-      for (int i = 0; i < 4; ++i) dst[i] = v[i];
-    }
+    for (int i = 0; i < 4; ++i) dst[i] = v[i];
   }
 }
 
+// Byte offset of 16-byte chunk c of row r in a 128B-swizzled tile.
+__device__ __forceinline__ uint32_t sw128_off(int r, int c) { return (uint32_t)r * 128u + (uint32_t)((c ^ (r & 7)) << 4); }
+
 __global__ void __launch_bounds__(kThreads, 1)
-k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CUtensorMap w_map, ConvArgs a) {
+k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CUtensorMap w_map,
+         const __grid_constant__ CUtensorMap out_map, const __grid_constant__ CUtensorMap z_map, ConvArgs a) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte aligned carve-up
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  unsigned char* sB = base;                          // 9 x 8 KB weights
-  unsigned char* sA = base + 9 * kBBytes;            // kStages x 16640 B row slabs
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sA + kStages * kSlabBytes + kSmemGuard);
+  unsigned char* sB = base;                                   // 9 x 8 KB weights
+  unsigned char* sA = sB + 9 * kBBytes;                       // kStages row slabs
+  unsigned char* sO = sA + kStages * kSlabStride;             // staging: halo'd output tile
+  unsigned char* sZ = sO + kStageTile;                        // staging: pre-activation tile
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sZ + kStageTile);
   uint64_t* full = bars;                 // [kStages]
   uint64_t* empty = bars + kStages;      // [kStages]
   uint64_t* acc_full = bars + 2 * kStages;   // [2]
@@ -210,7 +234,7 @@ k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CU
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
-                 "r"(128));
+                 "r"(512));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
   }
   tc_fence_before();
@@ -236,7 +260,7 @@ k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CU
           // padded row y + dy, padded columns xt*128 .. xt*128 + 129
           const int q = (b * (a.H + 2) + (y + dy)) * (a.W + 2) + xt * kTileM;
           mbar_expect_tx(&full[s], kSlabBytes);
-          tma_load_3d(sA + s * kSlabBytes, &act_map, &full[s], 0, q, 0);
+          tma_load_2d(sA + s * kSlabStride, &act_map, &full[s], 0, q);
         }
       }
       if (!ok) {
@@ -255,20 +279,20 @@ k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CU
         const uint32_t aph = (tcount >> 1) & 1;
         if (tcount >= 2 && !mbar_wait(&acc_empty[acc], aph ^ 1)) { ok = false; break; }
         tc_fence_after();
-        const uint32_t d = tmem + acc * 64;
+        const uint32_t d = tmem + acc * 256;  // accumulator k at d + 64 k
         for (int dy = 0; dy < 3 && ok; ++dy, ++it) {
           const int s = it % kStages;
           const uint32_t ph = (it / kStages) & 1;
           if (!mbar_wait(&full[s], ph)) { ok = false; break; }
           tc_fence_after();
-          const uint64_t ad = slab_desc(sA + s * kSlabBytes);
 #pragma unroll
           for (int dx = 0; dx < 3; ++dx) {
             const int t = 3 * dy + dx;
+            const uint64_t ad = slab_desc(sA + s * kSlabStride, dx);
             const uint64_t bd = sw128_desc(sB + t * kBBytes);
 #pragma unroll
-            for (int k = 0; k < 4; ++k)  // K = 16 channels: two core matrices (2 LBO) per MMA
-              umma(d, ad + dx + 2 * k * kSlabPix, bd + 2 * k, (t > 0 || k > 0) ? 1u : 0u);
+            for (int k = 0; k < 4; ++k)  // K = 16 per MMA: 32 bytes along the 128-byte row
+              umma(d + 64 * k, ad + 2 * k, bd + 2 * k, t > 0 ? 1u : 0u);
           }
           umma_commit(&empty[s]);  // frees the slab when these MMAs complete
         }
@@ -283,29 +307,36 @@ k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CU
     }
   } else {
     // ---------------- epilogue (warps 2..9) ----------------
-    const int quarter = warp & 3;  // TMEM lane quarter this warp may access
+    const int quarter = warp & 3;           // TMEM lane quarter this warp may access
     const int c0 = ((warp - 2) >> 2) * 32;  // its 32 accumulator columns
-    const int row = quarter * 32 + lane;
+    const int row = quarter * 32 + lane;    // pixel of the tile
+    const bool leader = (warp == 2 && lane == 0);
     float bz[32];
 #pragma unroll
     for (int i = 0; i < 32; ++i) bz[i] = (a.mode == CLOSURE_EPI_DGRAD) ? 0.f : a.bias[c0 + i];
     int tcount = 0;
-    for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x, ++tcount) {
+    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++tcount) {
       const int acc = tcount & 1;
       const uint32_t aph = (tcount >> 1) & 1;
-      if (!mbar_wait(&acc_full[acc], aph)) { ok = false; break; }
+      const int bad = mbar_wait(&acc_full[acc], aph) ? 0 : 1;
+      if (leader) bulk_wait_read_all();  // the staging tiles are free again
+      if (epi_sync_or(bad)) { ok = false; break; }
       tc_fence_after();
       float v[32];
-      uint32_t r[32];
-      const uint32_t taddr = tmem + acc * 64 + c0 + ((uint32_t)(quarter * 32) << 16);
-      TC_LD32(taddr, r);
-      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-      for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]) + bz[i];
+      for (int i = 0; i < 32; ++i) v[i] = bz[i];
+      const uint32_t taddr = tmem + acc * 256 + c0 + ((uint32_t)(quarter * 32) << 16);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        uint32_t r[32];
+        TC_LD32(taddr + 64 * k, r);
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] += __uint_as_float(r[i]);
+      }
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&acc_empty[acc]);
-      // pixel of this thread
       const int xt = tile % tiles_per_row;
       const int rowi = tile / tiles_per_row;
       const int y = rowi % a.H, b = rowi / a.H;
@@ -327,9 +358,8 @@ k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CU
           reinterpret_cast<__nv_bfloat162*>(zp)[i] = zb;
           reinterpret_cast<__nv_bfloat162*>(packed)[i] = __floats2bfloat162_rn(gelu(zr.x), gelu(zr.y));
         }
-        uint4* oz = reinterpret_cast<uint4*>(a.out_z + pix * kC + c0);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) oz[i] = zp[i];
+        for (int i = 0; i < 4; ++i) *reinterpret_cast<uint4*>(sZ + sw128_off(row, (c0 >> 3) + i)) = zp[i];
       } else {  // DGRAD
         const uint4* zsrc = reinterpret_cast<const uint4*>(a.zprev + pix * kC + c0);
         uint4 zq[4];
@@ -342,15 +372,29 @@ k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CU
               __floats2bfloat162_rn(v[2 * i] * gelu_grad(z.x), v[2 * i + 1] * gelu_grad(z.y));
         }
       }
-      store_halo(a.out_pad, a.H, a.W, b, y, x, c0, packed);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) *reinterpret_cast<uint4*>(sO + sw128_off(row, (c0 >> 3) + i)) = packed[i];
+      fence_async_smem();
+      epi_sync();
+      if (leader) {
+        const int Wp = a.W + 2;
+        const int xq = xt * kTileM + 1;  // padded column of the tile's first pixel
+        tma_store_2d(&out_map, sO, 0, (b * (a.H + 2) + y + 1) * Wp + xq);
+        if (y == 0) tma_store_2d(&out_map, sO, 0, (b * (a.H + 2) + a.H + 1) * Wp + xq);
+        if (y == a.H - 1) tma_store_2d(&out_map, sO, 0, (b * (a.H + 2)) * Wp + xq);
+        if (a.mode == CLOSURE_EPI_FWD) tma_store_2d(&z_map, sZ, 0, (b * a.H + y) * a.W + xt * kTileM);
+        bulk_commit();
+      }
+      if (x == 0 || x == a.W - 1) store_xhalo(a.out_pad, a.H, a.W, b, y, x, c0, packed);
     }
+    if (leader) bulk_wait_all();
     if (!ok) atomicOr(a.err, 4u);
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(128));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(512));
   }
 }
 
@@ -455,10 +499,11 @@ k_wgrad64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ C
         if (!mbar_wait(&full[s], ph)) { ok = false; break; }
         tc_fence_after();
         unsigned char* st = base + s * kWStageBytes;
+        // the five accumulators interleave, so consecutive MMAs are independent
 #pragma unroll
-        for (int m = 0; m < 5; ++m) {
+        for (int k = 0; k < 4; ++k) {  // K = 16 pixel rows = two 1024 B atoms
 #pragma unroll
-          for (int k = 0; k < 4; ++k) {  // K = 16 pixel rows = two 1024 B atoms
+          for (int m = 0; m < 5; ++m) {
             const uint64_t ad = sw128_mn_desc(st + (2 * m) * kWSlot, kWSlot) + 128 * k;
             const uint64_t bd = sw128_mn_desc(st + 10 * kWSlot, kWSlot) + 128 * k;
             umma_mn(tmem + m * 64, ad, bd, (it > 0 || k > 0) ? 1u : 0u);
@@ -548,22 +593,7 @@ bool make_map(CUtensorMap* m, const void* ptr, uint64_t rows, uint32_t box_rows)
            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// Halo'd activations as [rows][8 channel groups][8 channels]: box = 8
-// channels x 130 pixels x 8 groups, written unswizzled, channel group
-// outermost (the slab layout of slab_desc).
-bool make_slab_map(CUtensorMap* m, const void* ptr, uint64_t rows) {
-  PFN_encodeTiled f = encode_fn();
-  if (!f) return false;
-  cuuint64_t dims[3] = {8, rows, 8};
-  cuuint64_t strides[2] = {kC * 2, 16};
-  cuuint32_t box[3] = {8, (cuuint32_t)kSlabPix, 8};
-  cuuint32_t estr[3] = {1, 1, 1};
-  return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(ptr), dims, strides, box, estr,
-           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
-
-constexpr size_t kSmemBytes = 1024 + 9 * kBBytes + kStages * kSlabBytes + kSmemGuard + 256;
+constexpr size_t kSmemBytes = 1024 + 9 * kBBytes + kStages * kSlabStride + 2 * kStageTile + 256;
 
 }  // namespace
 
@@ -581,10 +611,18 @@ int closure_conv64(int32_t B, int32_t H, int32_t W, int32_t mode, const void* ac
   if (mode == CLOSURE_EPI_FWD && (!bias || !out_pad || !out_z)) return cfail(1, "closure_conv64: FWD needs bias, out_pad, out_z");
   if (mode == CLOSURE_EPI_DGRAD && (!zprev || !out_pad)) return cfail(1, "closure_conv64: DGRAD needs zprev, out_pad");
   if (mode == CLOSURE_EPI_LIN && (!bias || !out_f32)) return cfail(1, "closure_conv64: LIN needs bias, out_f32");
-  CUtensorMap amap, wmap;
+  if (mode != CLOSURE_EPI_LIN && (((uintptr_t)out_pad % 16) || (out_z && (uintptr_t)out_z % 16)))
+    return cfail(1, "closure_conv64: output pointers must be 16-byte aligned");
+  CUtensorMap amap, wmap, omap, zmap;
   const uint64_t prows = (uint64_t)B * (H + 2) * (W + 2);
-  if (!make_slab_map(&amap, act_pad, prows) || !make_map(&wmap, weights, 9 * kC, kC))
+  if (!make_map(&amap, act_pad, prows, kSlabRows) || !make_map(&wmap, weights, 9 * kC, kC))
     return cfail(2, "closure_conv64: tensor map encoding failed");
+  omap = amap;  // unused in LIN mode
+  zmap = amap;  // unused unless FWD
+  if (mode != CLOSURE_EPI_LIN && !make_map(&omap, out_pad, prows, kTileM))
+    return cfail(2, "closure_conv64: tensor map encoding failed (output)");
+  if (mode == CLOSURE_EPI_FWD && !make_map(&zmap, out_z, (uint64_t)B * H * W, kTileM))
+    return cfail(2, "closure_conv64: tensor map encoding failed (pre-activation)");
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(k_conv64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes) != cudaSuccess)
@@ -595,13 +633,12 @@ int closure_conv64(int32_t B, int32_t H, int32_t W, int32_t mode, const void* ac
   a.B = B; a.H = H; a.W = W; a.mode = mode; a.bias = bias;
   a.zprev = (const __nv_bfloat16*)zprev;
   a.out_pad = (__nv_bfloat16*)out_pad;
-  a.out_z = (__nv_bfloat16*)out_z;
   a.out_f32 = out_f32;
   a.err = err;
   const int n_tiles = B * H * (W / kTileM);
   int g = grid > 0 ? grid : 148;
   if (g > n_tiles) g = n_tiles;
-  k_conv64<<<g, kThreads, kSmemBytes, (cudaStream_t)stream>>>(amap, wmap, a);
+  k_conv64<<<g, kThreads, kSmemBytes, (cudaStream_t)stream>>>(amap, wmap, omap, zmap, a);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cfail(2, std::string("closure_conv64 launch: ") + cudaGetErrorString(e));
   return 0;

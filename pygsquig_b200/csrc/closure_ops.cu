@@ -13,6 +13,7 @@
 #include <string>
 
 #include "../../include/sqg_closure.h"
+#include "closure_act.cuh"
 
 namespace {
 
@@ -22,10 +23,6 @@ int ofail(const std::string& m) {
   return 1;
 }
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
-__device__ __forceinline__ float gelu_grad(float z) {
-  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
-}
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 __device__ __forceinline__ size_t padidx(int b, int y, int x, int H, int W) {
   return ((size_t)b * (H + 2) + (y + 1)) * (W + 2) + (x + 1);
@@ -82,84 +79,114 @@ __device__ __forceinline__ float2 ld2(const __nv_bfloat16* t, size_t pix, int la
   return __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(t + pix * 64)[lane]);
 }
 
-// After the call lane l holds, in v[0], the sum over all lanes of their v[l].
-__device__ __forceinline__ float reduce_scatter32(float (&v)[32], int lane) {
-#pragma unroll
-  for (int off = 16; off >= 1; off >>= 1) {
-    const bool upper = (lane & off) != 0;
-#pragma unroll
-    for (int i = 0; i < off; ++i) {
-      const float send = upper ? v[i] : v[i + off];
-      const float keep = upper ? v[i + off] : v[i];
-      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, off);
-    }
+// The 8-channel variant of put2: lane group g owns channels 8g .. 8g+7.
+__device__ __forceinline__ void put8(__nv_bfloat16* out, int H, int W, int b, int y, int x, int g, uint4 v) {
+  const int Hp = H + 2, Wp = W + 2;
+  const int y2 = (y == 0) ? H + 1 : (y == H - 1 ? 0 : -1);
+  const int x2 = (x == 0) ? W + 1 : (x == W - 1 ? 0 : -1);
+  reinterpret_cast<uint4*>(out + (((size_t)b * Hp + y + 1) * Wp + x + 1) * 64)[g] = v;
+  if (y2 >= 0) reinterpret_cast<uint4*>(out + (((size_t)b * Hp + y2) * Wp + x + 1) * 64)[g] = v;
+  if (x2 >= 0) {
+    reinterpret_cast<uint4*>(out + (((size_t)b * Hp + y + 1) * Wp + x2) * 64)[g] = v;
+    if (y2 >= 0) reinterpret_cast<uint4*>(out + (((size_t)b * Hp + y2) * Wp + x2) * 64)[g] = v;
   }
-  return v[0];
+}
+
+__device__ __forceinline__ uint4 pack8(const float (&f)[8]) {
+  uint4 v;
+  __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&v);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
+  return v;
 }
 
 // Layer 1 forward: z = conv3x3(in_scale x; w[9][64]) + b (1 -> 64), a = gelu(z).
+// A warp takes its 32-pixel chunk four pixels at a time: lane l computes
+// pixel l / 8 of the four, channels 8 (l % 8) .. +7, and writes them as one
+// 16-byte store per tensor (a warp store covers 512 contiguous bytes).
 __global__ void __launch_bounds__(kWarps * 32) k_conv_in(int B, int H, int W, float in_scale, const float* __restrict__ x,
                                                          const float* __restrict__ w, const float* __restrict__ bias,
                                                          __nv_bfloat16* __restrict__ z, __nv_bfloat16* __restrict__ a_pad) {
   __shared__ float stg[kWarps][3][34];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float w0[9], w1[9];
+  const int sub = lane >> 3, g = lane & 7;
+  float wr[9][8], b8[8];
 #pragma unroll
-  for (int t = 0; t < 9; ++t) {
-    w0[t] = w[t * 64 + 2 * lane] * in_scale;
-    w1[t] = w[t * 64 + 2 * lane + 1] * in_scale;
-  }
-  const float b0 = bias[2 * lane], b1 = bias[2 * lane + 1];
+  for (int t = 0; t < 9; ++t)
+#pragma unroll
+    for (int i = 0; i < 8; ++i) wr[t][i] = w[t * 64 + 8 * g + i] * in_scale;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) b8[i] = bias[8 * g + i];
   const size_t n_chunks = (size_t)B * H * W / kChunk;
   for (size_t ch = (size_t)blockIdx.x * kWarps + warp; ch < n_chunks; ch += (size_t)gridDim.x * kWarps) {
     const Chunk c = chunk_of(ch, H, W);
     __syncwarp();
     stage_rows(stg[warp], x, H, W, c, lane);
-    for (int j = 0; j < kChunk; ++j) {
-      float s0 = b0, s1 = b1;
+#pragma unroll 2
+    for (int q = 0; q < kChunk / 4; ++q) {
+      const int j = 4 * q + sub;
+      float sv[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) sv[i] = b8[i];
 #pragma unroll
       for (int t = 0; t < 9; ++t) {
         const float xv = stg[warp][t / 3][j + t % 3];
-        s0 += xv * w0[t];
-        s1 += xv * w1[t];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) sv[i] += xv * wr[t][i];
       }
-      const __nv_bfloat162 zb = __floats2bfloat162_rn(s0, s1);
-      reinterpret_cast<__nv_bfloat162*>(z + (c.p0 + j) * 64)[lane] = zb;
-      const float2 zf = __bfloat1622float2(zb);
-      put2(a_pad, H, W, c.b, c.y, c.x0 + j, lane, __floats2bfloat162_rn(gelu(zf.x), gelu(zf.y)));
+      const uint4 zb = pack8(sv);
+      reinterpret_cast<uint4*>(z + (c.p0 + j) * 64)[g] = zb;
+      const __nv_bfloat162* zh = reinterpret_cast<const __nv_bfloat162*>(&zb);
+      float av[8];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const float2 zf = __bfloat1622float2(zh[i]);  // the stored pre-activation
+        av[2 * i] = gelu(zf.x);
+        av[2 * i + 1] = gelu(zf.y);
+      }
+      put8(a_pad, H, W, c.b, c.y, c.x0 + j, g, pack8(av));
     }
   }
 }
 
 // Last layer forward: y = out_scale (conv3x3(a; w[9][64]) + b) (64 -> 1), FP32.
+// Four pixels per warp step: lane l reads 8 channels (16 bytes) of pixel l / 8
+// per tap, and the eight lanes of a pixel add their partial sums by shuffles.
 __global__ void __launch_bounds__(kWarps * 32) k_conv_out(int B, int H, int W, float out_scale,
                                                           const __nv_bfloat16* __restrict__ a_pad,
                                                           const float* __restrict__ w, const float* __restrict__ bias,
                                                           float* __restrict__ y) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float w0[9], w1[9];
+  const int sub = lane >> 3, g = lane & 7;
+  float wr[9][8];
 #pragma unroll
-  for (int t = 0; t < 9; ++t) {
-    w0[t] = w[t * 64 + 2 * lane];
-    w1[t] = w[t * 64 + 2 * lane + 1];
-  }
+  for (int t = 0; t < 9; ++t)
+#pragma unroll
+    for (int i = 0; i < 8; ++i) wr[t][i] = w[t * 64 + 8 * g + i];
   const float bb = bias[0];
   const size_t n_chunks = (size_t)B * H * W / kChunk;
   for (size_t ch = (size_t)blockIdx.x * kWarps + warp; ch < n_chunks; ch += (size_t)gridDim.x * kWarps) {
     const Chunk c = chunk_of(ch, H, W);
-    float acc[kChunk];
-#pragma unroll
-    for (int j = 0; j < kChunk; ++j) {
-      float s = 0.f;
+#pragma unroll 2
+    for (int q = 0; q < kChunk / 4; ++q) {
+      const int j = 4 * q + sub;
+      float sacc = 0.f;
 #pragma unroll
       for (int t = 0; t < 9; ++t) {
-        const float2 f = ld2(a_pad, padidx(c.b, c.y + t / 3 - 1, c.x0 + j + t % 3 - 1, H, W), lane);
-        s += f.x * w0[t] + f.y * w1[t];
+        const uint4 v = reinterpret_cast<const uint4*>(
+            a_pad + padidx(c.b, c.y + t / 3 - 1, c.x0 + j + t % 3 - 1, H, W) * 64)[g];
+        const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const float2 f = __bfloat1622float2(h[i]);
+          sacc += f.x * wr[t][2 * i] + f.y * wr[t][2 * i + 1];
+        }
       }
-      acc[j] = s;
+      sacc += __shfl_xor_sync(0xffffffffu, sacc, 4);
+      sacc += __shfl_xor_sync(0xffffffffu, sacc, 2);
+      sacc += __shfl_xor_sync(0xffffffffu, sacc, 1);
+      if (g == 0) y[c.p0 + j] = (sacc + bb) * out_scale;
     }
-    const float tot = reduce_scatter32(acc, lane);
-    y[c.p0 + lane] = (tot + bb) * out_scale;
   }
 }
 

@@ -450,9 +450,11 @@ int check_ready(const sqg_plan* pl) {
 
 // One RK4 stage: column pass (with ring reduction) then row pass.
 int run_stage(sqg_plan* pl, int s, const void* th_n, void* th_out, double dt, const void* extra,
-              const double* phases, int stage_write, int do_p1, cudaStream_t st, RingCtl* ctl = nullptr) {
+              const double* phases, int stage_write, int do_p1, cudaStream_t st, RingCtl* ctl = nullptr,
+              const void* src_phys = nullptr) {
   KP kp = make_kp(pl, dt);
   ColArgs ca = base_col(pl);
+  ca.in_real = src_phys;
   if (ring_active(pl)) {
     if (!phases && !ctl) return fail(SQG_ERR_INVALID, "ring forcing needs phases");
     ring_args(pl, ca, s, s == 1 ? th_n : (const void*)(pl->ws + pl->off_stage), phases, dt, ctl);
@@ -692,6 +694,19 @@ int sqg_stage(sqg_plan* pl, int32_t s, const void* th_in, void* th_out, double d
   if (s < 1 || s > 4) return fail(SQG_ERR_INVALID, "stage must be 1..4");
   rc = run_stage(pl, s, th_in, th_out, dt, extra, phases, stage_write_mode(pl, true), s < 4 ? 1 : 0,
                  (cudaStream_t)stream);
+  if (s == 4) pl->stage_begun = false;
+  return rc;
+}
+
+int sqg_stage_physical(sqg_plan* pl, int32_t s, const void* th_in, void* th_out, double dt, const void* src,
+                       const double* phases, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!pl->stage_begun) return fail(SQG_ERR_STATE, "sqg_stage_physical before sqg_stage_begin");
+  if (s < 1 || s > 4) return fail(SQG_ERR_INVALID, "stage must be 1..4");
+  if (!src) return fail(SQG_ERR_INVALID, "null source field");
+  rc = run_stage(pl, s, th_in, th_out, dt, nullptr, phases, stage_write_mode(pl, true), s < 4 ? 1 : 0,
+                 (cudaStream_t)stream, nullptr, src);
   if (s == 4) pl->stage_begun = false;
   return rc;
 }
@@ -1486,7 +1501,6 @@ int sqg_batch_workspace_bytes(const sqg_batch* b, size_t* bytes) {
 int sqg_batch_set_workspace(sqg_batch* b, void* ws, size_t bytes, void* stream) {
   if (!b) return fail(SQG_ERR_INVALID, "null batch");
   if (!ws || bytes < b->off_total) return fail(SQG_ERR_WORKSPACE, "workspace missing or too small");
-  cudaStream_t st = (cudaStream_t)stream;
   // grid tables: the first bytes of the workspace, as a plan lays them out
   int rc = sqg_plan_set_workspace(&b->tables, ws, b->tables.off_acc, stream);
   if (rc != SQG_OK) return rc;
@@ -1509,7 +1523,6 @@ int sqg_batch_set_workspace(sqg_batch* b, void* ws, size_t bytes, void* stream) 
   if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
   b->args_dt = -1.0;
   b->ready = true;
-  (void)st;
   return SQG_OK;
 }
 

@@ -317,7 +317,6 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a) {
     }
     const int s = a.stage;
     const bool scal = a.fmode == FM_SCAL;
-    const C* th_n = reinterpret_cast<const C*>(a.th_n);
     const C* st_in = reinterpret_cast<const C*>(s == 1 ? a.th_n : a.st_in);
     C* acc = reinterpret_cast<C*>(a.acc);
     C* st_out = reinterpret_cast<C*>(a.st_out);
@@ -510,7 +509,7 @@ struct ColArgs {
   const void* uv;   // N x N complex u + i v (CM_SCAL input)
   void* out0;       // CM_VEL: u (real N x N) or uv complex; CM_PHYS1: real field
   void* out1;       // CM_VEL: v (real) ; null -> write complex uv into out0
-  const void* in_real;  // CM_FWD: real N x N field
+  const void* in_real;  // CM_FWD: real N x N field; CM_THETA: source subtracted from J (or null)
   // ring forcing reduction, run by the extra last CTA
   int ring_cta;
   int stage;
@@ -667,6 +666,15 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
       W[m].x = V[0][m].x * V[1][m].x + V[2][m].x * V[3][m].x;
       W[m].y = V[0][m].y * V[1][m].y + V[2][m].y * V[3][m].y;
     }
+    if (a.in_real) {  // physical-space source: J - src
+      const T* f = reinterpret_cast<const T*>(a.in_real);
+#pragma unroll
+      for (int m = 0; m < R; ++m) {
+        const size_t x = j + m * G;
+        W[m].x -= f[x * N + ya];
+        W[m].y -= f[x * N + ya + 1];
+      }
+    }
   } else {
     for (int rd = 0; rd < nround; ++rd) {
       if (rd == 1) {
@@ -699,6 +707,15 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
           W[m].y = w1.x * V[0][m].y + w1.y * V[1][m].y;
         }
       }
+    }
+  }
+  if (!(NBUF == 4 && nround == 2) && a.cmode == CM_THETA && a.in_real) {  // physical-space source: J - src
+    const T* f = reinterpret_cast<const T*>(a.in_real);
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+      const size_t x = j + m * G;
+      W[m].x -= f[x * N + ya];
+      W[m].y -= f[x * N + ya + 1];
     }
   }
   // forward DFT along x of Ja + i Jb
