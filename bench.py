@@ -287,6 +287,7 @@ def main():
 
     from oracle import sqg_oracle as O  # initial field generator (host, seeded)
     import pygsquig_b200 as P
+    from pygsquig_b200 import replicas
     from pygsquig_b200.build import build
 
     if rank == 0:
@@ -358,10 +359,8 @@ def main():
                 torch.cuda.synchronize()
             sampler.stop()
         ms = sum(a.elapsed_time(b) for a, b in evs)
+        ms = replicas.max_over_ranks(ms, "cuda")  # slowest rank
         if world > 1:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
             dist.barrier()
         th = st["theta_hat"]
         finite = bool(torch.isfinite(torch.view_as_real(th)).all().item())
@@ -391,10 +390,7 @@ def main():
             e1.record(stream)
             torch.cuda.synchronize()
             ems = e0.elapsed_time(e1)
-            if world > 1:
-                t = torch.tensor([ems], device="cuda", dtype=torch.float64)
-                dist.all_reduce(t, op=dist.ReduceOp.MAX)
-                ems = float(t.item())
+            ems = replicas.max_over_ranks(ems, "cuda")
             res["e2e"] = {"value": world * steps / (ems / 1e3), "unit": "steps/s",
                           "h2d_bytes_per_step": int(n_ring * 8), "d2h_bytes_per_step": 8}
         del flush
@@ -417,10 +413,7 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = replicas.max_over_ranks(ms, "cuda")
         finite = all(bool(torch.isfinite(torch.view_as_real(t)).all().item()) for t in ens.theta)
         n_scal = sum(len(m.scalars0) for m in members)
         return {"value": world * steps / (ms / 1e3), "unit": "ensemble steps/s",
