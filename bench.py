@@ -424,6 +424,65 @@ def main():
                           "nu=1e-6 p=8 dt=5e-4, one CUDA graph per size class per step, no L2 flush "
                           "(working set > L2)"}
 
+    def measure_closure(steps=300, warmup=20):
+        """Closure-vs-DNS GPU time per unit of simulated time: the coarse
+        N = 256 FP32 solve with the CNN closure on every RK stage (graph
+        replay, forcing split into DNS-sized sub-steps) against the N = 2048
+        FP32 DNS step (graph multistep), both with ring forcing kf = 20 and
+        CombinedDamping as in the closure experiment.  The spectral error
+        comes from the committed experiment report (its cost does not depend
+        on the weights)."""
+        import math
+
+        from pygsquig_b200.closure import experiment as X
+        from pygsquig_b200.closure.cnn import ClosureCNN
+        from pygsquig_b200.closure.model import ClosureSolver, SubgridClosure
+
+        cfg = X.Config()
+        here = os.path.join(ROOT, "pygsquig_b200", "closure", "trained")
+        wpath = os.path.join(here, "closure_weights.npz")
+        if os.path.exists(wpath):
+            clo = SubgridClosure.load(wpath)
+        else:
+            clo = SubgridClosure(ClosureCNN(cfg.N_c, cfg.N_c, max_batch=1), cfg.N_c, 2 * math.pi, 1.0, 1e-3)
+        m = int(round(cfg.dt_c / cfg.dt))
+        rng = np.random.default_rng(11)
+        out = {}
+        # coarse closure solve
+        g, s, damp, ring = X._solver(cfg, cfg.N_c, cfg.nu)
+        runner = ClosureSolver(s, clo, damp, ring, forcing_substeps=m)
+        st = s.initialize(theta0=rng.standard_normal((cfg.N_c, cfg.N_c)) * 0.3)
+        noise = torch.as_tensor(rng.uniform(0, 2 * math.pi, ((warmup + steps) * m, ring.n_modes(g))), device="cuda")
+        st = runner.multistep(st, warmup, cfg.dt_c, noise)
+        torch.cuda.synchronize()
+        tm = []
+        runner.multistep(st, steps, cfg.dt_c, noise[warmup * m:], timer=tm)
+        torch.cuda.synchronize()
+        coarse_ms = sum(a.elapsed_time(b) for a, b in tm) / steps
+        # DNS step
+        gf, sf, dampf, ringf = X._solver(cfg, cfg.N_dns, cfg.nu)
+        stf = sf.initialize(theta0=rng.standard_normal((cfg.N_dns, cfg.N_dns)) * 0.3)
+        nf = 100
+        noisef = torch.as_tensor(rng.uniform(0, 2 * math.pi, (nf + 10, ringf.n_modes(gf))), device="cuda")
+        stf = sf.multistep(stf, 10, cfg.dt, forcing=ringf, damping=dampf, noise=noisef[:10])
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sf.multistep(stf, nf, cfg.dt, forcing=ringf, damping=dampf, noise=noisef[10:])
+        e1.record()
+        torch.cuda.synchronize()
+        dns_ms = e0.elapsed_time(e1) / nf
+        out.update({"coarse_ms_per_step": coarse_ms, "coarse_dt": cfg.dt_c, "coarse_N": cfg.N_c,
+                    "dns_ms_per_step": dns_ms, "dns_dt": cfg.dt, "dns_N": cfg.N_dns,
+                    "gpu_time_ratio": (dns_ms / cfg.dt) / (coarse_ms / cfg.dt_c),
+                    "forcing_substeps": m, "weights": "trained" if os.path.exists(wpath) else "random (timing only)"})
+        rpath = os.path.join(here, "closure_report.json")
+        if os.path.exists(rpath):
+            r = json.load(open(rpath))["models"]["closure"]
+            out["max_rel_err_E_k_le_kf"] = r["max_rel_err_E_k_le_kf"]
+            out["error_source"] = "pygsquig_b200/closure/trained/closure_report.json"
+        return out
+
     if args.workload == "ensemble96":
         r = measure_ensemble(args.steps, args.warmup)
         if rank == 0:
@@ -491,6 +550,8 @@ def main():
                                                 for k, (m, c) in v["kernels"].items() if c}}
     if args.variants == "auto":
         line["variant_ensemble96"] = measure_ensemble(200, 10)
+    if args.variants == "auto":
+        line["closure_vs_dns"] = measure_closure()
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

@@ -99,6 +99,28 @@ int sqg_plan_buffer(const sqg_plan* plan, int32_t which, size_t* offset, size_t*
 int sqg_ring_mode_count(const sqg_plan* plan, int32_t* n_ring);
 int sqg_ring_modes(const sqg_plan* plan, int32_t* ix, int32_t* iy);
 
+/* Split forcing (an extension for coarse solves whose step is larger than
+ * the step the forcing statistics were set with): n_sub forcing-only RK4
+ * sub-steps of length dt_sub on the ring modes of theta_hat, in place, each
+ * with its own row of phases (device float64[n_sub][n_ring]).  Each sub-step
+ * is the RK4 step of d theta/dt = s(<theta F>) F with the reference's rescale
+ * s(r) = eps / r (ring_forcing.py:151-170), computed exactly through the
+ * linearity of <theta F> in theta.  White-in-time forcing only (tau_f = 0). */
+int sqg_ring_substeps(sqg_plan* plan, void* theta_hat, int32_t n_sub, double dt_sub, const double* phases,
+                      void* stream);
+
+/* Launch shapes of the transform passes (an extension; the reference has no
+ * kernels to shape).  The row pass runs rpc row pairs per CTA and the column
+ * pass np column pairs per CTA, each a power-of-two divisor of a compiled
+ * maximum (0 selects the maximum).  The shape changes speed only: every
+ * transform is computed the same way, so results are bit-identical across
+ * shapes.  sqg_plan_autotune times the passes of one right-hand side for
+ * every shape on the plan's own workspace (which must be set) and keeps the
+ * fastest; it synchronises the stream. */
+int sqg_plan_shape(const sqg_plan* plan, int32_t* rpc, int32_t* np, int32_t* max_rpc, int32_t* max_np);
+int sqg_plan_set_shape(sqg_plan* plan, int32_t rpc, int32_t np);
+int sqg_plan_autotune(sqg_plan* plan, int32_t reps, void* stream);
+
 /* Core RHS -fft2(jacobian) + hyperviscosity(nu_p) of theta_hat
  * (replaces _compute_core_rhs, pygsquig/core/solver.py:28-58). */
 int sqg_rhs(sqg_plan* plan, const void* theta_hat, void* rhs, void* stream);

@@ -81,6 +81,10 @@ SIGNATURES = {
     "sqg_stage_begin": [_vp, _vp, _vp],
     "sqg_stage": [_vp, _i32, _vp, _vp, _dbl, _vp, _vp, _vp],
     "sqg_stage_physical": [_vp, _i32, _vp, _vp, _dbl, _vp, _vp, _vp],
+    "sqg_plan_shape": [_vp, _vp, _vp, _vp, _vp],
+    "sqg_plan_set_shape": [_vp, _i32, _i32],
+    "sqg_plan_autotune": [_vp, _i32, _vp],
+    "sqg_ring_substeps": [_vp, _vp, _i32, _dbl, _vp, _vp],
     "sqg_velocity": [_vp, _vp, _vp, _vp, _vp],
     "sqg_to_physical": [_vp, _vp, _vp, _vp],
     "sqg_to_spectral": [_vp, _vp, _vp, _vp],

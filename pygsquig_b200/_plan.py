@@ -256,6 +256,31 @@ class Plan:
         arr_out = (C.c_void_p * max(n, 1))(*[t.data_ptr() for t in s_out])
         _lib.check(self._lib.sqg_scalars_step(self._h, th_new.data_ptr(), arr_in, arr_out, float(dt), _stream_ptr()))
 
+    def ring_substeps(self, th, n_sub, dt_sub, phases):
+        """n_sub forcing-only RK4 sub-steps on the ring modes of th (in place);
+        phases: device float64 [n_sub, n_ring]."""
+        _lib.check(self._lib.sqg_ring_substeps(self._h, th.data_ptr(), int(n_sub), float(dt_sub), _ptr(phases),
+                                               _stream_ptr()))
+
+    # ---- launch shapes ----
+    def shape(self) -> dict:
+        """Current and maximal launch shapes: row pairs per CTA of the row
+        pass (rpc) and column pairs per CTA of the column pass (np)."""
+        v = [C.c_int32() for _ in range(4)]
+        _lib.check(self._lib.sqg_plan_shape(self._h, *[C.byref(x) for x in v]))
+        return {"rpc": v[0].value, "np": v[1].value, "max_rpc": v[2].value, "max_np": v[3].value}
+
+    def set_shape(self, rpc: int = 0, np_: int = 0) -> None:
+        """Select launch shapes (0: the compiled maximum).  Results are
+        bit-identical for every shape."""
+        _lib.check(self._lib.sqg_plan_set_shape(self._h, int(rpc), int(np_)))
+
+    def autotune(self, reps: int = 5) -> dict:
+        """Time every launch shape on this plan's workspace and keep the
+        fastest (synchronises the current stream)."""
+        _lib.check(self._lib.sqg_plan_autotune(self._h, int(reps), _stream_ptr()))
+        return self.shape()
+
     def check_status(self) -> int:
         f = C.c_uint32()
         _lib.check(self._lib.sqg_check_status(self._h, C.byref(f), _stream_ptr()))
@@ -281,6 +306,9 @@ class Plan:
 
 _CACHE: dict = {}
 
+# Plans pick their launch shapes by timing them when they are created.
+AUTOTUNE = True
+
 
 def get_plan(key: PlanKey) -> Plan:
     dev = torch.cuda.current_device() if torch.cuda.is_available() else -1
@@ -288,6 +316,8 @@ def get_plan(key: PlanKey) -> Plan:
     pl = _CACHE.get(k)
     if pl is None:
         pl = Plan(key)
+        if AUTOTUNE:
+            pl.autotune()
         _CACHE[k] = pl
     return pl
 

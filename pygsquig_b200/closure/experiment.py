@@ -84,6 +84,7 @@ class Config:
     batch: int = 16
     lr: float = 1e-3
     val_frac: float = 0.05
+    k_low: float = 40.0  # cut-off of the low-pass subgrid target (2 kf)
     train_seconds: float = 0.0  # > 0: stop training after this wall time
 
 
@@ -166,6 +167,10 @@ def generate(cfg: Config, log=print):
     per_run = cfg.pairs // cfg.runs
     X = torch.empty((per_run * cfg.runs, Nc, Nc), dtype=torch.float32, device="cuda")
     Y = torch.empty_like(X)
+    Yl = torch.empty_like(X)  # low-pass part |k| <= k_low of the subgrid term
+    from .spectral import _kmag
+
+    low = (_kmag(Nc, TWO_PI, "cuda") <= cfg.k_low).to(torch.complex64)
     stats = _Stats(shell.n_shell)
     run_E = []
     ke = []
@@ -203,6 +208,7 @@ def generate(cfg: Config, log=print):
             j = r * per_run + i
             nl_c.to_physical(thc, out=X[j])
             nl_c.to_physical(pi_hat, out=Y[j])
+            nl_c.to_physical(pi_hat * low, out=Yl[j])
         # evaluation window: filtered spectra and transfer
         ics.append(filt(st["theta_hat"]).clone())
         rs = _Stats(shell.n_shell)
@@ -224,7 +230,7 @@ def generate(cfg: Config, log=print):
         "E": stats.mean()[0], "T": stats.mean()[1], "run_E": np.array(run_E), "ke_mean": float(np.mean(ke)),
         "ms_per_step": ms / n_dns_steps, "steps": n_dns_steps, "spin_log": spin_log,
     }
-    return X, Y, ics, dns
+    return X, (Y, Yl), ics, dns
 
 
 def train(cfg: Config, X, Y, log=print):
@@ -299,21 +305,41 @@ def validate(net, X, Y, idx, sig_t, sig_p, max_n=256):
     return {"val_rel_mse": num / den, "val_corr": dot / math.sqrt(den * ny + 1e-300)}
 
 
-def evaluate(cfg: Config, closure: SubgridClosure, ics, dns, log=print):
+def variants(cfg: Config, closures: dict):
+    """Coarse solves compared with the filtered DNS: name -> (nu, closure,
+    dt, forcing sub-steps per step).  ``closures``: "full" (the CNN trained
+    on the whole subgrid term, run with the DNS hyperviscosity) and "low"
+    (trained on its |k| <= k_low part, run with the grid-scaled
+    hyperviscosity that drains the smallest resolved scales).  The split
+    forcing keeps the DNS's forcing step (dt_c / m = dt); the last two runs
+    show the closure with the forcing inside the coarse RK stages, and a
+    plain coarse solve at the DNS step."""
+    Nc = cfg.N_c
+    m = max(1, int(round(cfg.dt_c / cfg.dt)))
+    v = {
+        "closure": (cfg.nu, closures.get("full"), cfg.dt_c, m),
+        "closure_lowpass_grid_nu": (_nu_at(cfg, Nc), closures.get("low"), cfg.dt_c, m),
+        "no_closure": (cfg.nu, None, cfg.dt_c, m),
+        "no_closure_grid_nu": (_nu_at(cfg, Nc), None, cfg.dt_c, m),
+        "closure_forcing_in_stages": (cfg.nu, closures.get("full"), cfg.dt_c, 0),
+        "no_closure_grid_nu_dns_dt": (_nu_at(cfg, Nc), None, cfg.dt, 0),
+    }
+    return {k: x for k, x in v.items() if not (x[1] is None and k.startswith("closure"))}
+
+
+def evaluate(cfg: Config, closures: dict, ics, dns, log=print, only=None):
     Nc = cfg.N_c
     shell = ShellSpectrum(Nc, TWO_PI, cfg.alpha)
     nl_c = get_plan(PlanKey(N=Nc, L=TWO_PI, alpha=cfg.alpha, nu_p=0.0, p=cfg.p, precision="float32", role="aux"))
-    n_per = int(round(cfg.sample_dt / cfg.dt_c))
     n_samples = int(round(cfg.t_eval / cfg.sample_dt))
-    variants = {
-        "closure": (cfg.nu, closure),
-        "no_closure": (cfg.nu, None),
-        "no_closure_grid_nu": (_nu_at(cfg, Nc), None),
-    }
     out = {}
-    for name, (nu, clo) in variants.items():
+    for name, (nu, clo, dt_c, m) in variants(cfg, closures).items():
+        if only and name not in only:
+            continue
+        n_per = int(round(cfg.sample_dt / dt_c))
         g, s, damp, ring = _solver(cfg, Nc, nu)
-        runner = ClosureSolver(s, clo, damp, ring)
+        runner = ClosureSolver(s, clo, damp, ring, forcing_substeps=m)
+        rows = runner.noise_rows_per_step
         stats = _Stats(shell.n_shell)
         timer = []
         diverged = False
@@ -321,22 +347,21 @@ def evaluate(cfg: Config, closure: SubgridClosure, ics, dns, log=print):
             st = {"theta_hat": ic.clone(), "time": 0.0, "step": 0}
             noise = _Noise(30_000 + r, ring.n_modes(g))
             for i in range(n_samples):
-                if clo is not None:
-                    st = runner.multistep(st, n_per, cfg.dt_c, noise.take(n_per), timer=timer)
-                else:
-                    st = _run_steps(s, st, n_per, cfg.dt_c, ring, damp, noise, timer)
+                st = runner.multistep(st, n_per, dt_c, noise.take(n_per * rows), timer=timer)
                 th = st["theta_hat"]
                 tend = runner.tendency(th, nl_c)
                 stats.add(shell.energy(th), shell.transfer(th, tend))
-            if not bool(torch.isfinite(st["theta_hat"]).all().item()):
+            if not bool(torch.isfinite(torch.view_as_real(st["theta_hat"])).all().item()):
                 diverged = True
         E, T = stats.mean()
         steps = len(ics) * n_samples * n_per
         ms = _elapsed_ms(timer)
-        out[name] = {"E": E, "T": T, "ms_per_step": ms / steps, "steps": steps, "diverged": diverged}
-        log(f"[eval] {name}: {ms / steps:.4f} ms/step diverged={diverged}")
-    if closure.errors():
-        raise RuntimeError("closure kernels reported a timed-out wait")
+        out[name] = {"E": E, "T": T, "ms_per_step": ms / steps, "steps": steps, "diverged": diverged, "dt": dt_c,
+                     "forcing_substeps": m}
+        log(f"[eval] {name}: {ms / steps:.4f} ms/step dt={dt_c} substeps={m} diverged={diverged}")
+    for clo in closures.values():
+        if clo is not None and clo.errors():
+            raise RuntimeError("closure kernels reported a timed-out wait")
     return out
 
 
@@ -398,6 +423,9 @@ def report(cfg: Config, dns, train_info, ev, out_dir):
         "shells": list(range(1, kf + 1)),
         "E_dns": dns["E"][1:kf + 1].tolist(),
         "flux_dns": flux(dns["T"])[1:kf + 1].tolist(),
+        "E_dns_rel_sem": (np.std(dns["run_E"][:, 1:kf + 1], axis=0, ddof=1) /
+                          np.mean(dns["run_E"][:, 1:kf + 1], axis=0) / math.sqrt(len(dns["run_E"]))).tolist()
+        if len(dns["run_E"]) > 1 else None,
         "dns_run_spread_max": float(np.max(np.std(dns["run_E"][:, 1:kf + 1], axis=0) /
                                            np.mean(dns["run_E"][:, 1:kf + 1], axis=0) / math.sqrt(cfg.runs))),
         "spin_log": dns["spin_log"],
@@ -410,8 +438,10 @@ def report(cfg: Config, dns, train_info, ev, out_dir):
         rel_all = spectral_errors(m["E"], dns["E"], nres - 1)
         rep["models"][name] = {
             "ms_per_step": m["ms_per_step"],
-            "ms_per_unit_time": m["ms_per_step"] / cfg.dt_c,
-            "speedup_vs_dns": dns_ms_per_time / (m["ms_per_step"] / cfg.dt_c),
+            "dt": m["dt"],
+            "forcing_substeps": m["forcing_substeps"],
+            "ms_per_unit_time": m["ms_per_step"] / m["dt"],
+            "speedup_vs_dns": dns_ms_per_time / (m["ms_per_step"] / m["dt"]),
             "E": m["E"][1:kf + 1].tolist(),
             "rel_err_E": rel.tolist(),
             "max_rel_err_E_k_le_kf": float(np.max(rel)),
@@ -432,10 +462,17 @@ def main(argv=None):
     ap.add_argument("--out", default="closure_out")
     ap.add_argument("--calibrate", action="store_true", help="one short run of each stage (timings, statistics)")
     ap.add_argument("--set", nargs="*", default=[], help="Config overrides name=value")
+    ap.add_argument("--eval-from", default=None,
+                    help="directory of an earlier run: reuse its DNS statistics, initial states and weights")
+    ap.add_argument("--only", nargs="*", default=None, help="evaluate only these coarse variants")
     a = ap.parse_args(argv)
     cfg = Config()
     if a.calibrate:
         cfg = Config(runs=1, pairs=400, t_spin=10.0, t_adjust=0.2, t_eval=0.5, epochs=2, pair_stride=10)
+    if a.eval_from:
+        with open(os.path.join(a.eval_from, "closure_report.json")) as f:
+            for k, v in json.load(f)["config"].items():
+                setattr(cfg, k, v)
     for kv in a.set:
         k, v = kv.split("=")
         setattr(cfg, k, type(getattr(cfg, k))(v))
@@ -445,21 +482,44 @@ def main(argv=None):
     build()
     log = lambda *m: print(*m, flush=True)  # noqa: E731
     t0 = time.time()
-    X, Y, ics, dns = generate(cfg, log)
-    log(f"[dns] {dns['ms_per_step']:.4f} ms/step, KE {dns['ke_mean']:.4f}, wall {time.time() - t0:.0f} s")
-    net, tinfo, val_idx = train(cfg, X, Y, log)
-    tinfo["cnn_timing"] = time_cnn(net)
-    log(f"[train] cnn timing {tinfo['cnn_timing']}")
-    closure = SubgridClosure(net, cfg.N_c, TWO_PI, tinfo["sigma_theta"], tinfo["sigma_pi"])
     os.makedirs(a.out, exist_ok=True)
-    closure.save(os.path.join(a.out, "closure_weights.npz"), config=asdict(cfg))
-    ev = evaluate(cfg, closure, ics, dns, log)
+    if a.eval_from:
+        z = np.load(os.path.join(a.eval_from, "dns.npz"), allow_pickle=False)
+        dns = {k: z[k] for k in z.files}
+        dns["ke_mean"] = float(dns["ke_mean"])
+        dns["ms_per_step"] = float(dns["ms_per_step"])
+        dns["steps"] = int(dns["steps"])
+        dns["spin_log"] = dns["spin_log"].tolist()
+        ics = [torch.as_tensor(c).cuda() for c in np.load(os.path.join(a.eval_from, "ics.npz"))["ics"]]
+        closures = {"full": SubgridClosure.load(os.path.join(a.eval_from, "closure_weights.npz"))}
+        lp = os.path.join(a.eval_from, "closure_weights_lowpass.npz")
+        if os.path.exists(lp):
+            closures["low"] = SubgridClosure.load(lp)
+        with open(os.path.join(a.eval_from, "closure_report.json")) as f:
+            tinfo = json.load(f)["training"]
+        val_idx = None
+    else:
+        X, (Y, Yl), ics, dns = generate(cfg, log)
+        log(f"[dns] {dns['ms_per_step']:.4f} ms/step, KE {dns['ke_mean']:.4f}, wall {time.time() - t0:.0f} s")
+        np.savez(os.path.join(a.out, "dns.npz"), **{k: np.asarray(v) for k, v in dns.items()})
+        np.savez_compressed(os.path.join(a.out, "ics.npz"), ics=torch.stack(ics).cpu().numpy())
+        net, tinfo, val_idx = train(cfg, X, Y, log)
+        tinfo["cnn_timing"] = time_cnn(net)
+        log(f"[train] cnn timing {tinfo['cnn_timing']}")
+        closures = {"full": SubgridClosure(net, cfg.N_c, TWO_PI, tinfo["sigma_theta"], tinfo["sigma_pi"])}
+        closures["full"].save(os.path.join(a.out, "closure_weights.npz"), config=asdict(cfg))
+        net_l, tinfo_l, _ = train(cfg, X, Yl, log)
+        closures["low"] = SubgridClosure(net_l, cfg.N_c, TWO_PI, tinfo_l["sigma_theta"], tinfo_l["sigma_pi"])
+        closures["low"].save(os.path.join(a.out, "closure_weights_lowpass.npz"), config=asdict(cfg), target="lowpass")
+        tinfo["lowpass"] = tinfo_l
+    ev = evaluate(cfg, closures, ics, dns, log, only=a.only)
     rep = report(cfg, dns, tinfo, ev, a.out)
-    # small fixtures: validation pairs, one coarse initial state, the DNS spectrum
-    vi = val_idx[:4]
-    np.savez_compressed(os.path.join(a.out, "closure_fixture.npz"), theta=X[vi].cpu().numpy(),
-                        pi=Y[vi].cpu().numpy(), ic=ics[-1].cpu().numpy(), E_dns=dns["E"],
-                        T_dns=dns["T"])
+    if val_idx is not None:
+        # small fixtures: validation pairs, one coarse initial state, the DNS spectrum
+        vi = val_idx[:4]
+        np.savez_compressed(os.path.join(a.out, "closure_fixture.npz"), theta=X[vi].cpu().numpy(),
+                            pi=Y[vi].cpu().numpy(), ic=ics[-1].cpu().numpy(), E_dns=dns["E"],
+                            T_dns=dns["T"])
     summ = {k: {kk: v[kk] for kk in ("max_rel_err_E_k_le_kf", "speedup_vs_dns", "mean_rel_err_E_all_resolved",
                                      "diverged")} for k, v in rep["models"].items()}
     log(json.dumps({"eddy_time": rep["eddy_time"], "models": summ}))

@@ -102,28 +102,51 @@ class SubgridClosure:
 
 
 class ClosureSolver:
-    """Coarse gSQG solve with fused ring forcing / damping plus a learned
-    closure on every RK stage; ``multistep`` captures one step (4 closure
-    evaluations and 4 fused stages) in a CUDA graph and replays it."""
+    """Coarse gSQG solve with ring forcing / damping plus a learned closure on
+    every RK stage; ``multistep`` captures one step (4 closure evaluations and
+    4 fused stages) in a CUDA graph and replays it.
+
+    ``forcing_substeps = m > 0`` splits the ring forcing off the RK stages:
+    each step of length dt applies m forcing-only RK4 sub-steps of dt / m
+    (half before the stages, half after; Strang splitting), each with its own
+    phases (sqg_ring_substeps).  The reference's rescaled white-noise forcing
+    injects an amount of energy that depends on the step it is integrated
+    with (the rescale eps / <theta F> is singular where the overlap crosses
+    zero), so a coarse solve whose step is m times the DNS step sees the DNS's
+    forcing statistics only when the forcing keeps the DNS step.
+    """
 
     def __init__(self, solver, closure: Optional[SubgridClosure], damping: Optional[CombinedDamping] = None,
-                 ring: Optional[RingForcing] = None):
+                 ring: Optional[RingForcing] = None, forcing_substeps: int = 0):
         if solver.scheme != "ifrk4" and solver.scheme != "explicit":
             raise ValueError("unknown scheme")
+        if forcing_substeps and ring is None:
+            raise ValueError("forcing_substeps needs a RingForcing")
         self.solver, self.closure, self.damping, self.ring = solver, closure, damping, ring
-        self.pl = solver.plan(damping, ring)
+        self.m = int(forcing_substeps)
+        self.pl = solver.plan(damping, None if self.m else ring)
+        self.pl_ring = solver.plan(damping, ring) if ring is not None else None
         N = solver.grid.N
         dev = self.pl.device
+        self.n_ring = self.pl_ring.n_ring if self.pl_ring is not None else 0
         self.th_a = torch.zeros((N, N), dtype=self.pl.cdtype, device=dev)
         self.th_b = torch.zeros_like(self.th_a)
-        self.ph = torch.zeros(max(self.pl.n_ring, 1), dtype=torch.float64, device=dev)
+        self.ph = torch.zeros((max(self.m, 1), max(self.n_ring, 1)), dtype=torch.float64, device=dev)
         self.graph = None
         self.graph_dt = None
+
+    @property
+    def noise_rows_per_step(self) -> int:
+        """Rows of ring phases one step consumes (m with split forcing, else 1)."""
+        return max(self.m, 1)
 
     def _body(self, dt):
         pl = self.pl
         stage_buf = pl.buffer(_lib.SQG_BUF_STAGE, self.th_a.dtype, self.th_a.shape)
-        ph = self.ph if self.ring is not None else None
+        ph = self.ph[0] if (self.ring is not None and not self.m) else None
+        m1 = self.m // 2
+        if self.m:
+            self.pl_ring.ring_substeps(self.th_a, m1, dt / self.m, self.ph[:m1])
         pl.stage_begin(self.th_a)
         for s in range(1, 5):
             th_s = self.th_a if s == 1 else stage_buf
@@ -132,6 +155,8 @@ class ClosureSolver:
             else:
                 pl.stage(s, self.th_a, self.th_b, dt, None, ph)
         self.th_a.copy_(self.th_b)
+        if self.m:
+            self.pl_ring.ring_substeps(self.th_a, self.m - m1, dt / self.m, self.ph[m1:])
 
     def _capture(self, dt):
         cur = torch.cuda.current_stream()
@@ -149,11 +174,13 @@ class ClosureSolver:
 
     def multistep(self, state: dict, n_steps: int, dt: float, noise: Optional[torch.Tensor] = None,
                   timer: Optional[list] = None) -> dict:
-        """n_steps steps; ``noise``: device float64 [n_steps, n_ring] ring
-        phases.  ``timer`` (a list) receives (start, end) CUDA events around
-        the replays."""
-        if self.ring is not None and (noise is None or noise.shape[0] < n_steps):
-            raise ValueError("ring forcing needs noise of shape (n_steps, n_ring)")
+        """n_steps steps; ``noise``: device float64 ring phases, one row per
+        step ([n_steps, n_ring]), or m rows per step with split forcing
+        ([n_steps * m, n_ring]).  ``timer`` (a list) receives (start, end)
+        CUDA events around the replays."""
+        rows = self.noise_rows_per_step
+        if self.ring is not None and (noise is None or noise.shape[0] < n_steps * rows):
+            raise ValueError(f"ring forcing needs noise of shape ({n_steps * rows}, n_ring)")
         self.th_a.copy_(self.pl.check_spectrum(state["theta_hat"]))
         if self.graph is None or self.graph_dt != dt:
             self._capture(dt)
@@ -164,7 +191,7 @@ class ClosureSolver:
             ev[0].record()
         for i in range(n_steps):
             if self.ring is not None:
-                self.ph.copy_(noise[i])
+                self.ph.copy_(noise[i * rows:(i + 1) * rows])
             self.graph.replay()
         if ev is not None:
             ev[1].record()

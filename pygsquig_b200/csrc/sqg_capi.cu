@@ -55,6 +55,7 @@ struct sqg_plan {
   int n_src_buf;
   bool ready = false;
   bool stage_begun = false;
+  int rpc = 0, np = 0;  // launch shapes of the row / column passes (0: compiled maximum)
   int64_t launches = 0;
   // CUDA graph of one steady-state step (multistep)
   cudaGraphExec_t graph_exec = nullptr;
@@ -302,19 +303,34 @@ size_t col_smem() {
          sizeof(typename Cplx<T>::type);
 }
 
+// Launch shapes: a.rpc row pairs per CTA of the row pass (a.np column pairs
+// per CTA of the column pass), a power-of-two divisor of the compiled maximum;
+// shared memory scales with it.  Results do not depend on the shape (every
+// row and column transform is computed the same way); only the number and
+// size of the CTAs change.
 template <typename T, int L>
 cudaError_t launch_row_t(const KP& kp, const RowArgs& a, cudaStream_t st) {
   constexpr int N = 1 << L, RPC = rows_per_cta<T, L>();
-  const int grid = (N / 2 + 1 + RPC - 1) / RPC;
-  k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()><<<grid, RPC * row_group<T, L>(), row_smem<T, L>(), st>>>(kp, a);
+  const int rpc = a.rpc > 0 ? a.rpc : RPC;
+  const int grid = (N / 2 + 1 + rpc - 1) / rpc;
+  k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>
+      <<<grid, rpc * row_group<T, L>(), row_smem<T, L>() / RPC * rpc, st>>>(kp, a);
   return cudaGetLastError();
 }
 template <typename T, int L>
 cudaError_t launch_col_t(const KP& kp, const ColArgs& a, cudaStream_t st, bool ring_only) {
   constexpr int N = 1 << L, NP = pairs_per_cta<T, L>();
-  int grid = ring_only ? 1 : N / (2 * NP) + (a.ring_cta ? 1 : 0);
-  k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()><<<grid, NP * col_group<T, L>(), col_smem<T, L>(), st>>>(kp, a);
+  const int np = a.np > 0 ? a.np : NP;
+  int grid = ring_only ? 1 : N / (2 * np) + (a.ring_cta ? 1 : 0);
+  k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()>
+      <<<grid, np * col_group<T, L>(), col_smem<T, L>() / NP * np, st>>>(kp, a);
   return cudaGetLastError();
+}
+template <typename T, int L>
+cudaError_t shape_max_t(int* rpc, int* np) {
+  *rpc = rows_per_cta<T, L>();
+  *np = pairs_per_cta<T, L>();
+  return cudaSuccess;
 }
 template <typename T, int L>
 cudaError_t set_attrs_t() {
@@ -352,6 +368,10 @@ cudaError_t launch_col_p(int log2n, const KP& kp, const ColArgs& a, cudaStream_t
 template <typename T>
 cudaError_t set_attrs_p(int log2n) {
   SQG_DISPATCH(log2n, set_attrs_t);
+}
+template <typename T>
+cudaError_t shape_max_p(int log2n, int* rpc, int* np) {
+  SQG_DISPATCH(log2n, shape_max_t, rpc, np);
 }
 
 // Timing kinds reported by sqg_timing_read.
@@ -403,6 +423,7 @@ RowArgs base_row(sqg_plan* pl) {
   a.st_in = pl->ws + pl->off_stage;
   a.st_out = pl->ws + pl->off_stage;
   a.fmode = FM_THETA;
+  a.rpc = pl->rpc;
   return a;
 }
 
@@ -412,6 +433,7 @@ ColArgs base_col(sqg_plan* pl) {
   a.cmode = CM_THETA;
   a.xh = pl->ws + pl->off_xh;
   a.jh = pl->ws + pl->off_jh;
+  a.np = pl->np;
   return a;
 }
 
@@ -646,6 +668,99 @@ int sqg_plan_host_tables(const sqg_plan* pl, double* k1d, int32_t* dmax, int32_t
     if (dragmax) dragmax[i] = pl->rows[i].dragmax;
   }
   return SQG_OK;
+}
+
+int sqg_plan_shape(const sqg_plan* pl, int32_t* rpc, int32_t* np, int32_t* max_rpc, int32_t* max_np) {
+  if (!pl) return fail(SQG_ERR_INVALID, "null plan");
+  int mr = 0, mn = 0;
+  if (pl->d.precision == SQG_F64) shape_max_p<double>(pl->log2N, &mr, &mn);
+  else shape_max_p<float>(pl->log2N, &mr, &mn);
+  if (rpc) *rpc = pl->rpc > 0 ? pl->rpc : mr;
+  if (np) *np = pl->np > 0 ? pl->np : mn;
+  if (max_rpc) *max_rpc = mr;
+  if (max_np) *max_np = mn;
+  return SQG_OK;
+}
+
+int sqg_plan_set_shape(sqg_plan* pl, int32_t rpc, int32_t np) {
+  if (!pl) return fail(SQG_ERR_INVALID, "null plan");
+  int mr = 0, mn = 0;
+  if (pl->d.precision == SQG_F64) shape_max_p<double>(pl->log2N, &mr, &mn);
+  else shape_max_p<float>(pl->log2N, &mr, &mn);
+  auto ok = [](int v, int m) { return v == 0 || (v >= 1 && v <= m && (m % v) == 0 && (v & (v - 1)) == 0); };
+  if (!ok(rpc, mr)) return fail(SQG_ERR_INVALID, "rpc must be 0 or a power-of-two divisor of " + std::to_string(mr));
+  if (!ok(np, mn)) return fail(SQG_ERR_INVALID, "np must be 0 or a power-of-two divisor of " + std::to_string(mn));
+  if (pl->rpc != rpc || pl->np != np) {
+    pl->rpc = rpc;
+    pl->np = np;
+    if (pl->graph_exec) {  // the captured step holds the old launch shapes
+      cudaGraphExecDestroy(pl->graph_exec);
+      pl->graph_exec = nullptr;
+    }
+  }
+  return SQG_OK;
+}
+
+// Times the transform passes of one right-hand side (row inverse pass,
+// column pass, row pass) for every launch shape on the plan's own buffers and
+// keeps the fastest.  Blocks the calling thread (events are synchronised).
+int sqg_plan_autotune(sqg_plan* pl, int32_t reps, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (reps < 1) reps = 1;
+  cudaStream_t st = (cudaStream_t)stream;
+  int mr = 0, mn = 0;
+  if (pl->d.precision == SQG_F64) shape_max_p<double>(pl->log2N, &mr, &mn);
+  else shape_max_p<float>(pl->log2N, &mr, &mn);
+  void* th = pl->ws + pl->off_state;  // scratch input (zeroed) and output inside the workspace
+  void* out = pl->ws + pl->off_stage;
+  const size_t full = (size_t)pl->N * pl->N * pl->csize;
+  SQG_CUDA(cudaMemsetAsync(th, 0, full, st));
+  const bool timing = pl->timing;
+  pl->timing = false;
+  const int r0 = pl->rpc, n0 = pl->np;
+  auto one = [&]() -> int {
+    int e = run_p1(pl, th, FM_THETA, nullptr, st);
+    if (e) return e;
+    KP kp = make_kp(pl, 0.0);
+    kp.ring_on = 0;
+    ColArgs ca = base_col(pl);
+    SQG_CUDA(launch_col(pl, kp, ca, st));
+    RowArgs ra = base_row(pl);
+    ra.rmode = RM_RHS;
+    ra.stage = 1;
+    ra.th_n = th;
+    ra.rhs_out = out;
+    ra.do_p1 = 0;
+    SQG_CUDA(launch_row(pl, kp, ra, st));
+    return SQG_OK;
+  };
+  cudaEvent_t e0, e1;
+  SQG_CUDA(cudaEventCreate(&e0));
+  SQG_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int br = 0, bn = 0;
+  for (int r = mr; r >= 1 && rc == SQG_OK; r /= 2) {
+    for (int n = mn; n >= 1 && rc == SQG_OK; n /= 2) {
+      pl->rpc = r;
+      pl->np = n;
+      if ((rc = one()) != SQG_OK) break;  // warm-up
+      cudaEventRecord(e0, st);
+      for (int k = 0; k < reps && rc == SQG_OK; ++k) rc = one();
+      cudaEventRecord(e1, st);
+      if (cudaEventSynchronize(e1) != cudaSuccess) { rc = fail(SQG_ERR_CUDA, "autotune: event"); break; }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) { best = ms; br = r; bn = n; }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  pl->timing = timing;
+  pl->rpc = r0;
+  pl->np = n0;
+  if (rc != SQG_OK) return rc;
+  return sqg_plan_set_shape(pl, br == mr ? 0 : br, bn == mn ? 0 : bn);
 }
 
 int sqg_rhs(sqg_plan* pl, const void* theta, void* rhs, void* stream) {
@@ -887,6 +1002,32 @@ int sqg_ring_forcing(sqg_plan* pl, const void* theta, const double* phases, doub
   else
     k_ring_scatter<float><<<(n + 255) / 256, 256, 0, st>>>(n, wsp<int>(pl, pl->off_ring_pos), kp.ringF, (float2*)out);
   SQG_CUDA(cudaGetLastError());
+  return SQG_OK;
+}
+
+int sqg_ring_substeps(sqg_plan* pl, void* theta, int32_t n_sub, double dt_sub, const double* phases, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!theta) return fail(SQG_ERR_INVALID, "null pointer");
+  if (!ring_active(pl)) return fail(SQG_ERR_INVALID, "the plan carries no ring forcing");
+  if (pl->d.ring_tau_f > 0.0) return fail(SQG_ERR_INVALID, "forcing sub-steps need tau_f = 0 (white-in-time forcing)");
+  if (n_sub < 0) return fail(SQG_ERR_INVALID, "n_sub must be >= 0");
+  if (n_sub == 0) return SQG_OK;
+  if (!phases) return fail(SQG_ERR_INVALID, "forcing sub-steps need phases");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n = (int)pl->ring_pos.size();
+  const int4 ho = make_int4(pl->herm_ord[0], pl->herm_ord[1], pl->herm_ord[2], pl->herm_ord[3]);
+  double2* F = wsp<double2>(pl, pl->off_ringF);  // scratch: first n entries of the stage forcing table
+  const int* pos = wsp<int>(pl, pl->off_ring_pos);
+  const int* mir = wsp<int>(pl, pl->off_ring_mirror);
+  if (pl->d.precision == SQG_F64)
+    k_ring_substeps<double><<<1, 256, 0, st>>>(pl->N, n, pos, mir, ho, pl->d.ring_amplitude, pl->d.ring_epsilon, n_sub,
+                                               dt_sub, phases, (double2*)theta, F);
+  else
+    k_ring_substeps<float><<<1, 256, 0, st>>>(pl->N, n, pos, mir, ho, pl->d.ring_amplitude, pl->d.ring_epsilon, n_sub,
+                                              dt_sub, phases, (float2*)theta, F);
+  SQG_CUDA(cudaGetLastError());
+  pl->launches++;
   return SQG_OK;
 }
 

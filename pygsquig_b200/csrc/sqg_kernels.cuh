@@ -85,6 +85,7 @@ struct RowArgs {
   int n_src;
   void* src_out[4];
   double gx[4], gy[4];
+  int rpc;                        // row pairs per CTA (0: the compiled maximum RPC)
 };
 
 // ---- asynchronous global -> shared copies (cp.async) ----
@@ -246,8 +247,9 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a) {
   constexpr int XB = spad_size<R>(N);  // one exchange buffer
   C* wbuf = smem + (size_t)grp * NFX * XB;  // NFX exchange buffers of this group
   // prefetch staging: DEPTH chunks x 4 slots (theta_n e1/e2, acc e1/e2) x G
-  C* pf = smem + (size_t)RPC * NFX * XB + (size_t)grp * (DEPTH * 4 * G);
-  const int p_raw = blockIdx.x * RPC + grp;
+  const int rpc = a.rpc > 0 ? a.rpc : RPC;  // launch shape (autotuned), <= RPC
+  C* pf = smem + (size_t)rpc * NFX * XB + (size_t)grp * (DEPTH * 4 * G);
+  const int p_raw = blockIdx.x * rpc + grp;
   const bool valid = p_raw <= H;
   const int p = valid ? p_raw : H;
   const int pp = (N - p) & (N - 1);
@@ -525,6 +527,7 @@ struct ColArgs {
   int ring_ou;
   int herm_ord[4];          // ordinals of (0,0),(N/2,0),(0,N/2),(N/2,N/2) or -1
   double* ring_scale_out;   // [4]
+  int np;                   // column pairs per CTA (0: the compiled maximum NP)
 };
 
 // Slots of one field buffer of a column group: the raw half columns
@@ -536,13 +539,13 @@ template <int N, int R> struct ColBuf { static constexpr int SZ = spad_size<R>(N
 // the block into buffer slot `buf` of each group (no registers, no wait).
 template <typename T, int LOG2N, int R, int NP, int NBUF>
 __device__ __forceinline__ void col_fetch(const typename Cplx<T>::type* __restrict__ f, int y0, int buf,
-                                          typename Cplx<T>::type* smem) {
+                                          typename Cplx<T>::type* smem, int np) {
   using C = typename Cplx<T>::type;
-  constexpr int N = 1 << LOG2N, H = N / 2, G = N / R, NT = NP * G, SZ = ColBuf<N, R>::SZ;
-  constexpr int TOTAL = (H + 1) * NP * 2;
-  for (int idx = threadIdx.x; idx < TOTAL; idx += NT) {
-    const int c = idx % (2 * NP);      // column within the block (fastest: coalesced rows)
-    const int kx = idx / (2 * NP);
+  constexpr int N = 1 << LOG2N, H = N / 2, SZ = ColBuf<N, R>::SZ;
+  const int total = (H + 1) * np * 2;
+  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    const int c = idx % (2 * np);      // column within the block (fastest: coalesced rows)
+    const int kx = idx / (2 * np);
     const int q = c >> 1, b = c & 1;
     C* z = smem + (size_t)(q * NBUF + buf) * SZ;
     cp_async_elem(z + b * (H + 1) + kx, f + (size_t)kx * N + y0 + c, (int)sizeof(C));
@@ -589,7 +592,8 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
   const int grp = threadIdx.x / G;
   const int j = threadIdx.x - grp * G;
   C* gbuf = smem + (size_t)grp * NBUF * SZ;  // this group's NBUF buffers
-  const int y0 = blockIdx.x * (2 * NP);
+  const int np = a.np > 0 ? a.np : NP;       // launch shape (autotuned), <= NP
+  const int y0 = blockIdx.x * (2 * np);
   const int ya = y0 + 2 * grp;
   const C* __restrict__ tw = reinterpret_cast<const C*>(kp.tw);
   const C* xh = reinterpret_cast<const C*>(a.xh);
@@ -598,7 +602,7 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
 
   if (a.cmode == CM_VEL || a.cmode == CM_PHYS1) {
     const int nf = a.cmode == CM_VEL ? 2 : 1;
-    for (int f = 0; f < nf; ++f) col_fetch<T, LOG2N, R, NP, NBUF>(xh + f * fstride, y0, f, smem);
+    for (int f = 0; f < nf; ++f) col_fetch<T, LOG2N, R, NP, NBUF>(xh + f * fstride, y0, f, smem, np);
     cp_async_commit();
     cp_async_wait<0>();
     __syncthreads();
@@ -637,11 +641,11 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
   const int nround = a.cmode == CM_THETA ? 2 : (a.cmode == CM_SCAL ? 1 : 0);
   const int fa0 = 0, fb0 = a.cmode == CM_THETA ? 2 : 1, fa1 = 1, fb1 = 3;
   if (nround > 0) {
-    col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa0 * fstride, y0, 0, smem);
-    col_fetch<T, LOG2N, R, NP, NBUF>(xh + fb0 * fstride, y0, 1, smem);
+    col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa0 * fstride, y0, 0, smem, np);
+    col_fetch<T, LOG2N, R, NP, NBUF>(xh + fb0 * fstride, y0, 1, smem, np);
     if (NBUF == 4 && nround == 2) {
-      col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa1 * fstride, y0, 2, smem);
-      col_fetch<T, LOG2N, R, NP, NBUF>(xh + fb1 * fstride, y0, 3, smem);
+      col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa1 * fstride, y0, 2, smem, np);
+      col_fetch<T, LOG2N, R, NP, NBUF>(xh + fb1 * fstride, y0, 3, smem, np);
     }
     cp_async_commit();
   }
@@ -679,8 +683,8 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
     for (int rd = 0; rd < nround; ++rd) {
       if (rd == 1) {
         __syncthreads();  // round-1 buffers free
-        col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa1 * fstride, y0, 0, smem);
-        col_fetch<T, LOG2N, R, NP, NBUF>(xh + fb1 * fstride, y0, 1, smem);
+        col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa1 * fstride, y0, 0, smem, np);
+        col_fetch<T, LOG2N, R, NP, NBUF>(xh + fb1 * fstride, y0, 1, smem, np);
         cp_async_commit();
       }
       cp_async_wait<0>();
@@ -727,10 +731,10 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
   __syncthreads();
   // split: Ja(kx) = (W(kx) + conj W(-kx))/2, Jb(kx) = -i (W(kx) - conj W(-kx))/2
   C* jh = reinterpret_cast<C*>(a.jh);
-  const int total = (H + 1) * NP;
+  const int total = (H + 1) * np;
   for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    const int kx = idx / NP;
-    const int q = idx - kx * NP;
+    const int kx = idx / np;
+    const int q = idx - kx * np;
     const C* w = smem + (size_t)q * NBUF * SZ;
     const C wk = w[spad<R>(kx)];
     const C wm = w[spad<R>((N - kx) & (N - 1))];
@@ -783,25 +787,29 @@ __device__ void ring_reduce(const KP& kp, const ColArgs& a) {
     }
   }
   __syncthreads();
-  // 2. rate
+  // 2. rate: 256 fixed summation lanes (lane v sums modes v, v + 256, ...),
+  // then a tree over the lanes -- the same order whatever the block size
+  constexpr int V = 256;
   const C* th = reinterpret_cast<const C*>(a.ring_theta);
-  double acc = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const int pos = a.ring_pos[i];
-    const int ix = pos >> LOG2N, iy = pos & (N - 1);
-    const int mpos = (((N - ix) & (N - 1)) << LOG2N) | ((N - iy) & (N - 1));
-    const C t1 = th[pos], t2 = th[mpos];
-    const double hx = 0.5 * ((double)t1.x + (double)t2.x);
-    const double hy = 0.5 * ((double)t1.y - (double)t2.y);
-    const double2 f1 = F[i], f2 = F[a.ring_mirror[i]];
-    const double fx = 0.5 * (f1.x + f2.x);
-    const double fy = 0.5 * (f1.y - f2.y);
-    acc += hx * fx + hy * fy;
+  for (int v = threadIdx.x; v < V; v += blockDim.x) {
+    double acc = 0.0;
+    for (int i = v; i < n; i += V) {
+      const int pos = a.ring_pos[i];
+      const int ix = pos >> LOG2N, iy = pos & (N - 1);
+      const int mpos = (((N - ix) & (N - 1)) << LOG2N) | ((N - iy) & (N - 1));
+      const C t1 = th[pos], t2 = th[mpos];
+      const double hx = 0.5 * ((double)t1.x + (double)t2.x);
+      const double hy = 0.5 * ((double)t1.y - (double)t2.y);
+      const double2 f1 = F[i], f2 = F[a.ring_mirror[i]];
+      const double fx = 0.5 * (f1.x + f2.x);
+      const double fy = 0.5 * (f1.y - f2.y);
+      acc += hx * fx + hy * fy;
+    }
+    red[v] = acc;
   }
-  red[threadIdx.x] = acc;
   __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+  for (int w = V / 2; w > 0; w >>= 1) {
+    for (int v = threadIdx.x; v < w; v += blockDim.x) red[v] += red[v + w];
     __syncthreads();
   }
   if (threadIdx.x == 0) {

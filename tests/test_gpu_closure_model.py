@@ -85,3 +85,30 @@ def test_graph_replayed_closure_step_matches_eager_steps():
     c = plain["theta_hat"].cpu().numpy().astype(np.complex128)
     assert np.linalg.norm(a - c) / np.linalg.norm(c) > 1e-4
     assert clo.errors() == 0
+
+
+def test_forcing_substeps_match_forcing_only_rk4():
+    """sqg_ring_substeps against classic RK4 of d theta/dt = RingForcing(theta)
+    (the oracle's restatement of ring_forcing.py:119-170), three sub-steps."""
+    from oracle import sqg_oracle as O
+    from pygsquig_b200 import RingForcing, gSQGSolver, make_grid
+
+    N, dt = 64, 2e-3
+    g = make_grid(N, TWO_PI)
+    ring = RingForcing(8.0, 2.0, 0.1)
+    s = gSQGSolver(g, 1.0, 0.0, 8, precision="float64")
+    pl = s.plan(None, ring)
+    rng = np.random.default_rng(5)
+    th0 = _field_hat(N, 6) * 1e-2
+    phases = rng.uniform(0, TWO_PI, (3, ring.n_modes(g)))
+    th = torch.as_tensor(th0, dtype=torch.complex128, device="cuda").contiguous()
+    pl.ring_substeps(th, 3, dt, torch.as_tensor(phases, device="cuda"))
+    og = O.make_grid(N, TWO_PI)
+    ro = O.RingForcing(8.0, 2.0, 0.1)
+    ref = th0.copy()
+    for m in range(3):
+        ref = O.rk4_step(ref, lambda t: ro(t, phases[m], dt, og), dt)
+    got = th.cpu().numpy()
+    err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+    assert err < 1e-12, err
+    assert np.linalg.norm(got - th0) / np.linalg.norm(th0) > 1e-6  # the forcing acted
