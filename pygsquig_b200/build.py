@@ -14,6 +14,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -62,6 +63,7 @@ def up_to_date() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return OUT
+    t_start = time.time()
     os.makedirs(OBJ_DIR, exist_ok=True)
     objs = []
     for s in SRCS:
@@ -78,6 +80,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
     os.replace(OUT + ".tmp", OUT)
+    os.utime(OUT, (t_start, t_start))  # a source edited during the build makes the library stale
     return OUT
 
 

@@ -162,3 +162,47 @@ class ClosureCNN:
         for k, v in d.items():
             self.p[k].copy_(v.to(self.dev))
         self.refresh()
+
+
+def _main(argv=None) -> int:
+    """Time the network: python -m pygsquig_b200.closure.cnn [--batch B] [--reps R]
+    (CUDA events; forward at batch 1 and a training step at batch B)."""
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--reps", type=int, default=20)
+    a = ap.parse_args(argv)
+    from ..build import build
+
+    build()
+    net = ClosureCNN(a.size, a.size, max_batch=a.batch)
+    x1 = torch.randn(1, a.size, a.size, device="cuda")
+    xb = torch.randn(a.batch, a.size, a.size, device="cuda")
+    for _ in range(3):
+        net.forward(x1)
+        net.train_step(xb, xb, lr=0.0)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record()
+    for _ in range(a.reps):
+        net.forward(x1)
+    ev[1].record()
+    for _ in range(a.reps):
+        net.train_step(xb, xb, lr=0.0)
+    ev[2].record()
+    torch.cuda.synchronize()
+    if net.errors():
+        raise RuntimeError("closure kernels reported a timed-out wait")
+    fwd = ev[0].elapsed_time(ev[1]) / a.reps
+    trn = ev[1].elapsed_time(ev[2]) / a.reps
+    flop = 4 * 2 * 9 * 64 * 64 * a.size * a.size
+    print(json.dumps({"forward_ms_batch1": fwd, "train_step_ms": trn, "batch": a.batch,
+                      "forward_tensor_tflops": flop / fwd * 1e-9,
+                      "train_tensor_tflops": 3 * flop * a.batch / trn * 1e-9}))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(_main())

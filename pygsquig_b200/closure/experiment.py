@@ -324,6 +324,10 @@ def variants(cfg: Config, closures: dict):
         "closure_forcing_in_stages": (cfg.nu, closures.get("full"), cfg.dt_c, 0),
         "no_closure_grid_nu_dns_dt": (_nu_at(cfg, Nc), None, cfg.dt, 0),
     }
+    for g, (full, lowc) in closures.get("gains", {}).items():
+        v[f"closure_gain{g:g}"] = (cfg.nu, full, cfg.dt_c, m)
+        if lowc is not None:
+            v[f"closure_lowpass_grid_nu_gain{g:g}"] = (_nu_at(cfg, Nc), lowc, cfg.dt_c, m)
     return {k: x for k, x in v.items() if not (x[1] is None and k.startswith("closure"))}
 
 
@@ -359,7 +363,7 @@ def evaluate(cfg: Config, closures: dict, ics, dns, log=print, only=None):
         out[name] = {"E": E, "T": T, "ms_per_step": ms / steps, "steps": steps, "diverged": diverged, "dt": dt_c,
                      "forcing_substeps": m}
         log(f"[eval] {name}: {ms / steps:.4f} ms/step dt={dt_c} substeps={m} diverged={diverged}")
-    for clo in closures.values():
+    for clo in (closures.get("full"), closures.get("low")):
         if clo is not None and clo.errors():
             raise RuntimeError("closure kernels reported a timed-out wait")
     return out
@@ -465,6 +469,7 @@ def main(argv=None):
     ap.add_argument("--eval-from", default=None,
                     help="directory of an earlier run: reuse its DNS statistics, initial states and weights")
     ap.add_argument("--only", nargs="*", default=None, help="evaluate only these coarse variants")
+    ap.add_argument("--gains", default="", help="comma-separated output gains of extra closure variants")
     a = ap.parse_args(argv)
     cfg = Config()
     if a.calibrate:
@@ -512,6 +517,12 @@ def main(argv=None):
         closures["low"] = SubgridClosure(net_l, cfg.N_c, TWO_PI, tinfo_l["sigma_theta"], tinfo_l["sigma_pi"])
         closures["low"].save(os.path.join(a.out, "closure_weights_lowpass.npz"), config=asdict(cfg), target="lowpass")
         tinfo["lowpass"] = tinfo_l
+    gains = [float(x) for x in a.gains.split(",") if x]
+    if gains:
+        closures["gains"] = {
+            g: tuple(None if c is None else SubgridClosure(c.net, c.N, c.L, c.sigma_theta, c.sigma_pi * g, c.k_cut)
+                     for c in (closures["full"], closures.get("low")))
+            for g in gains}
     ev = evaluate(cfg, closures, ics, dns, log, only=a.only)
     rep = report(cfg, dns, tinfo, ev, a.out)
     if val_idx is not None:

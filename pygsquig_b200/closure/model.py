@@ -208,3 +208,48 @@ class ClosureSolver:
         if self.closure is not None:
             t = t + self.closure(theta_hat)
         return t
+
+
+def _main(argv=None) -> int:
+    """Time the coarse closure solve: python -m pygsquig_b200.closure.model
+    [--steps K] [--warmup W] [--no-closure] (graph replay, FP32 N = 256, the
+    trained network when present, forcing split into DNS-sized sub-steps)."""
+    import argparse
+    import json
+    import os
+
+    from .experiment import Config, _solver
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--no-closure", action="store_true")
+    a = ap.parse_args(argv)
+    from ..build import build
+
+    build()
+    cfg = Config()
+    w = os.path.join(os.path.dirname(os.path.abspath(__file__)), "trained", "closure_weights.npz")
+    clo = None
+    if not a.no_closure:
+        clo = (SubgridClosure.load(w) if os.path.exists(w)
+               else SubgridClosure(ClosureCNN(cfg.N_c, cfg.N_c, max_batch=1), cfg.N_c, 2 * math.pi, 1.0, 1e-3))
+    m = int(round(cfg.dt_c / cfg.dt))
+    g, s, damp, ring = _solver(cfg, cfg.N_c, cfg.nu)
+    runner = ClosureSolver(s, clo, damp, ring, forcing_substeps=m)
+    rng = np.random.default_rng(0)
+    st = s.initialize(theta0=rng.standard_normal((cfg.N_c, cfg.N_c)) * 0.3)
+    noise = torch.as_tensor(rng.uniform(0, 2 * math.pi, ((a.warmup + a.steps) * m, runner.n_ring)), device="cuda")
+    st = runner.multistep(st, a.warmup, cfg.dt_c, noise)
+    tm = []
+    st = runner.multistep(st, a.steps, cfg.dt_c, noise[a.warmup * m:], timer=tm)
+    torch.cuda.synchronize()
+    ms = sum(x.elapsed_time(y) for x, y in tm) / a.steps
+    print(json.dumps({"ms_per_step": ms, "closure": clo is not None, "N": cfg.N_c, "dt": cfg.dt_c,
+                      "forcing_substeps": m,
+                      "finite": bool(torch.isfinite(torch.view_as_real(st["theta_hat"])).all())}))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(_main())

@@ -79,6 +79,21 @@ __device__ __forceinline__ float2 ld2(const __nv_bfloat16* t, size_t pix, int la
   return __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(t + pix * 64)[lane]);
 }
 
+// After the call lane l holds, in v[0], the sum over all lanes of their v[l].
+__device__ __forceinline__ float reduce_scatter32(float (&v)[32], int lane) {
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) {
+    const bool upper = (lane & off) != 0;
+#pragma unroll
+    for (int i = 0; i < off; ++i) {
+      const float send = upper ? v[i] : v[i + off];
+      const float keep = upper ? v[i + off] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+    }
+  }
+  return v[0];
+}
+
 // The 8-channel variant of put2: lane group g owns channels 8g .. 8g+7.
 __device__ __forceinline__ void put8(__nv_bfloat16* out, int H, int W, int b, int y, int x, int g, uint4 v) {
   const int Hp = H + 2, Wp = W + 2;
@@ -150,43 +165,34 @@ __global__ void __launch_bounds__(kWarps * 32) k_conv_in(int B, int H, int W, fl
 }
 
 // Last layer forward: y = out_scale (conv3x3(a; w[9][64]) + b) (64 -> 1), FP32.
-// Four pixels per warp step: lane l reads 8 channels (16 bytes) of pixel l / 8
-// per tap, and the eight lanes of a pixel add their partial sums by shuffles.
 __global__ void __launch_bounds__(kWarps * 32) k_conv_out(int B, int H, int W, float out_scale,
                                                           const __nv_bfloat16* __restrict__ a_pad,
                                                           const float* __restrict__ w, const float* __restrict__ bias,
                                                           float* __restrict__ y) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int sub = lane >> 3, g = lane & 7;
-  float wr[9][8];
+  float w0[9], w1[9];
 #pragma unroll
-  for (int t = 0; t < 9; ++t)
-#pragma unroll
-    for (int i = 0; i < 8; ++i) wr[t][i] = w[t * 64 + 8 * g + i];
+  for (int t = 0; t < 9; ++t) {
+    w0[t] = w[t * 64 + 2 * lane];
+    w1[t] = w[t * 64 + 2 * lane + 1];
+  }
   const float bb = bias[0];
   const size_t n_chunks = (size_t)B * H * W / kChunk;
   for (size_t ch = (size_t)blockIdx.x * kWarps + warp; ch < n_chunks; ch += (size_t)gridDim.x * kWarps) {
     const Chunk c = chunk_of(ch, H, W);
-#pragma unroll 2
-    for (int q = 0; q < kChunk / 4; ++q) {
-      const int j = 4 * q + sub;
-      float sacc = 0.f;
+    float acc[kChunk];
+#pragma unroll
+    for (int j = 0; j < kChunk; ++j) {
+      float s = 0.f;
 #pragma unroll
       for (int t = 0; t < 9; ++t) {
-        const uint4 v = reinterpret_cast<const uint4*>(
-            a_pad + padidx(c.b, c.y + t / 3 - 1, c.x0 + j + t % 3 - 1, H, W) * 64)[g];
-        const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&v);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const float2 f = __bfloat1622float2(h[i]);
-          sacc += f.x * wr[t][2 * i] + f.y * wr[t][2 * i + 1];
-        }
+        const float2 f = ld2(a_pad, padidx(c.b, c.y + t / 3 - 1, c.x0 + j + t % 3 - 1, H, W), lane);
+        s += f.x * w0[t] + f.y * w1[t];
       }
-      sacc += __shfl_xor_sync(0xffffffffu, sacc, 4);
-      sacc += __shfl_xor_sync(0xffffffffu, sacc, 2);
-      sacc += __shfl_xor_sync(0xffffffffu, sacc, 1);
-      if (g == 0) y[c.p0 + j] = (sacc + bb) * out_scale;
+      acc[j] = s;
     }
+    const float tot = reduce_scatter32(acc, lane);
+    y[c.p0 + lane] = (tot + bb) * out_scale;
   }
 }
 

@@ -242,11 +242,13 @@ KP make_kp(const sqg_plan* pl, double dt) {
 }
 
 // ---- compile-time launch shapes ----
-// Radix of the group FFTs.  Column pass: 16 for float grids with N >= 1024
-// (groups of N/16 threads, fewer barrier rounds, two blocks per SM); row
-// pass: 8 (each thread walks R elements of the stage update).
+// Radix of the group FFTs.  Column pass: 16 for float grids with N >= 2048
+// (groups of N/16 threads, one exchange pass fewer, two 256-thread blocks per
+// SM; measured at N = 4096: 370 -> 271 us per launch); row pass: 8 (radix 16
+// with two exchange buffers made the fused stage pass slower, 384 -> 508 us,
+// because its stage update walks 16 prefetched chunks per thread).
 template <typename T, int L>
-constexpr int col_radix() { return 8; }
+constexpr int col_radix() { return (sizeof(T) == 4 && L >= 11) ? 16 : 8; }
 template <typename T, int L>
 constexpr int row_radix() { return 8; }
 template <typename T, int L>
@@ -261,18 +263,24 @@ constexpr int pairs_per_cta() {
   constexpr int cap = (1 << L) / 2 < 16 ? (1 << L) / 2 : 16;
   return g >= 256 ? 1 : (256 / g > cap ? cap : 256 / g);
 }
-// Four resident field buffers per column pair when they fit in 150 KB.
+// Four resident field buffers per column pair when they fit in 150 KB; the
+// radix-16 column pass (FP32, N >= 2048) keeps two (two rounds of two fields,
+// 256-thread blocks of about 67 KB, so that two or three blocks share an SM
+// and one block's loads overlap another's transforms).
 template <typename T, int L>
 constexpr int col_nbuf() {
-  return (size_t)pairs_per_cta<T, L>() * 4 * ColBuf<(1 << L), col_radix<T, L>()>::SZ *
-                     sizeof(typename Cplx<T>::type) <= 150 * 1024 ? 4 : 2;
+  return col_radix<T, L>() == 16 ? 2
+         : (size_t)pairs_per_cta<T, L>() * 4 * ColBuf<(1 << L), col_radix<T, L>()>::SZ *
+                       sizeof(typename Cplx<T>::type) <= 150 * 1024 ? 4 : 2;
 }
 // Exchange buffers of the row pass: four (the theta fields transform
-// together) when they fit in 150 KB, else two (two rounds).
+// together) when they fit in 150 KB, else two (two rounds); two for a
+// radix-16 row pass.
 template <typename T, int L>
 constexpr int row_nfx() {
-  return (size_t)rows_per_cta<T, L>() * 4 * spad_size<row_radix<T, L>()>(1 << L) * sizeof(typename Cplx<T>::type) <=
-                 150 * 1024 ? 4 : 2;
+  return row_radix<T, L>() == 16 ? 2
+         : (size_t)rows_per_cta<T, L>() * 4 * spad_size<row_radix<T, L>()>(1 << L) * sizeof(typename Cplx<T>::type) <=
+                   150 * 1024 ? 4 : 2;
 }
 template <typename T, int L>
 constexpr size_t row_base_smem() {
