@@ -11,6 +11,7 @@ not the objects does not rebuild.
 
 from __future__ import annotations
 
+import fcntl
 import os
 import subprocess
 import sys
@@ -63,6 +64,15 @@ def up_to_date() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return OUT
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    with open(os.path.join(OBJ_DIR, ".lock"), "w") as lock:
+        fcntl.flock(lock, fcntl.LOCK_EX)  # one build at a time (tests and scripts may race)
+        if not force and up_to_date():
+            return OUT
+        return _build(force, verbose)
+
+
+def _build(force: bool, verbose: bool) -> str:
     t_start = time.time()
     os.makedirs(OBJ_DIR, exist_ok=True)
     objs = []

@@ -291,17 +291,27 @@ template <typename T, int L>
 constexpr size_t row_pf_bytes(int depth) {
   return (size_t)rows_per_cta<T, L>() * depth * 4 * row_group<T, L>() * sizeof(typename Cplx<T>::type);
 }
-// Prefetch depth of the row pass: all R chunks when the block fits the budget
-// (220 KB when registers allow one block per SM anyway, else 110 KB), else
-// the largest power of two that fits.
+// Prefetch depth of the row pass: among R, R/2, R/4 and 1 chunks, the one
+// that lets the most blocks share an SM (the register budget's block count,
+// 227 KB of shared memory per SM with 1 KB reserved per block, at most 220 KB
+// per block), the deepest among equals: occupancy first, then prefetch depth.
+template <typename T, int L>
+constexpr int row_occupancy(int depth) {
+  constexpr int by_regs = min_blocks<T>(rows_per_cta<T, L>() * row_group<T, L>());
+  const size_t smem = row_base_smem<T, L>() + row_pf_bytes<T, L>(depth);
+  if (smem > 220 * 1024) return 0;
+  const int by_smem = (int)((227 * 1024) / (smem + 1024));
+  return by_smem < by_regs ? by_smem : by_regs;
+}
 template <typename T, int L>
 constexpr int row_depth() {
-  constexpr size_t budget = rows_per_cta<T, L>() * row_group<T, L>() >= 512 ? 220 * 1024 : 110 * 1024;
   constexpr int R = row_radix<T, L>();
-  return row_base_smem<T, L>() + row_pf_bytes<T, L>(R) <= budget       ? R
-         : row_base_smem<T, L>() + row_pf_bytes<T, L>(R / 2) <= budget ? R / 2
-         : row_base_smem<T, L>() + row_pf_bytes<T, L>(R / 4) <= budget ? R / 4
-                                                                       : 1;
+  int best = 1, occ = row_occupancy<T, L>(1);
+  for (int d = 2; d <= R; d *= 2) {
+    const int o = row_occupancy<T, L>(d);
+    if (o >= occ && o > 0) { occ = o; best = d; }
+  }
+  return best;
 }
 template <typename T, int L>
 size_t row_smem() { return row_base_smem<T, L>() + row_pf_bytes<T, L>(row_depth<T, L>()); }
