@@ -212,6 +212,13 @@ int sqg_ring_forcing(sqg_plan* plan, const void* theta_hat, const double* ring_p
 #define SQG_DIAG_COUNT 6
 int sqg_diagnostics(sqg_plan* plan, const void* theta_hat, double* out, void* stream);
 
+/* Maxima for adaptive time stepping (replace compute_max_velocity,
+ * pygsquig/core/adaptive_timestep.py:59-68, and the max |theta_hat| of the
+ * stability check, :288-305): out = device float64, NaN if any element is
+ * not finite.  u, v: real N x N of the plan precision. */
+int sqg_max_speed(sqg_plan* plan, const void* u, const void* v, double* out, void* stream);
+int sqg_spectrum_absmax(sqg_plan* plan, const void* theta_hat, double* out, void* stream);
+
 /* Shell energy spectrum E(k) (utils/diagnostics.py:31-84), n_bins =
  * min(N/4, 64) linear bins; out: device float64[n_bins]. */
 int sqg_energy_spectrum(sqg_plan* plan, const void* theta_hat, double* out, void* stream);

@@ -85,6 +85,8 @@ SIGNATURES = {
     "sqg_plan_set_shape": [_vp, _i32, _i32],
     "sqg_plan_autotune": [_vp, _i32, _vp],
     "sqg_ring_substeps": [_vp, _vp, _i32, _dbl, _vp, _vp],
+    "sqg_max_speed": [_vp, _vp, _vp, _vp, _vp],
+    "sqg_spectrum_absmax": [_vp, _vp, _vp, _vp],
     "sqg_velocity": [_vp, _vp, _vp, _vp, _vp],
     "sqg_to_physical": [_vp, _vp, _vp, _vp],
     "sqg_to_spectral": [_vp, _vp, _vp, _vp],

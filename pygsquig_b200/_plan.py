@@ -245,6 +245,18 @@ class Plan:
         _lib.check(self._lib.sqg_energy_spectrum(self._h, th.data_ptr(), out.data_ptr(), _stream_ptr()))
         return out.cpu().numpy()
 
+    def max_speed(self, u, v) -> float:
+        """max sqrt(u^2 + v^2) (NaN if a value is not finite)."""
+        out = torch.empty(1, dtype=torch.float64, device=self.device)
+        _lib.check(self._lib.sqg_max_speed(self._h, u.data_ptr(), v.data_ptr(), out.data_ptr(), _stream_ptr()))
+        return float(out.item())
+
+    def spectrum_absmax(self, th) -> float:
+        """max |theta_hat| (NaN if a value is not finite)."""
+        out = torch.empty(1, dtype=torch.float64, device=self.device)
+        _lib.check(self._lib.sqg_spectrum_absmax(self._h, th.data_ptr(), out.data_ptr(), _stream_ptr()))
+        return float(out.item())
+
     def scalar_variance(self, sh) -> float:
         out = torch.empty(1, dtype=torch.float64, device=self.device)
         _lib.check(self._lib.sqg_scalar_variance(self._h, sh.data_ptr(), out.data_ptr(), _stream_ptr()))

@@ -1,6 +1,8 @@
 // sqg_aux.cuh -- small kernels around the passes: damping term, ring-forcing
 // scatter, float64 diagnostics reductions, max |field|.
 #pragma once
+#include <math_constants.h>
+
 #include "sqg_kernels.cuh"
 
 namespace sqg {
@@ -318,5 +320,75 @@ __global__ void __launch_bounds__(256) k_ring_substeps(int N, int n, const int* 
     }
     __syncthreads();
   }
+}
+}  // namespace sqg
+
+namespace sqg {
+// Maxima for adaptive stepping (adaptive_timestep.py:59-68, 288-305): per
+// block, max sqrt(u^2 + v^2) of two real fields, or max |z| of a complex
+// field; a non-finite element makes the block's value NaN.  Max is
+// order-independent, so the result is deterministic.
+template <typename T>
+__global__ void k_speedmax_partial(const T* __restrict__ u, const T* __restrict__ v, size_t n, double* partial) {
+  __shared__ double sm[256];
+  double m = 0.0;
+  bool bad = false;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double a = (double)u[i], b = (double)v[i];
+    const double s = sqrt(a * a + b * b);
+    bad |= !isfinite(s);
+    m = fmax(m, s);
+  }
+  sm[threadIdx.x] = bad ? CUDART_NAN : m;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      const double x = sm[threadIdx.x], y = sm[threadIdx.x + w];
+      sm[threadIdx.x] = (isnan(x) || isnan(y)) ? CUDART_NAN : fmax(x, y);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sm[0];
+}
+template <typename C>
+__global__ void k_cabsmax_partial(const C* __restrict__ z, size_t n, double* partial) {
+  __shared__ double sm[256];
+  double m = 0.0;
+  bool bad = false;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double a = (double)z[i].x, b = (double)z[i].y;
+    const double s = sqrt(a * a + b * b);
+    bad |= !isfinite(s);
+    m = fmax(m, s);
+  }
+  sm[threadIdx.x] = bad ? CUDART_NAN : m;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      const double x = sm[threadIdx.x], y = sm[threadIdx.x + w];
+      sm[threadIdx.x] = (isnan(x) || isnan(y)) ? CUDART_NAN : fmax(x, y);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sm[0];
+}
+__global__ void k_nanmax_final(int nblocks, const double* partial, double* out) {
+  __shared__ double sm[256];
+  double m = 0.0;
+  bool bad = false;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+    bad |= isnan(partial[b]);
+    m = fmax(m, partial[b]);
+  }
+  sm[threadIdx.x] = bad ? CUDART_NAN : m;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      const double x = sm[threadIdx.x], y = sm[threadIdx.x + w];
+      sm[threadIdx.x] = (isnan(x) || isnan(y)) ? CUDART_NAN : fmax(x, y);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sm[0];
 }
 }  // namespace sqg

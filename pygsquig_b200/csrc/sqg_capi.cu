@@ -1049,6 +1049,38 @@ int sqg_ring_substeps(sqg_plan* pl, void* theta, int32_t n_sub, double dt_sub, c
   return SQG_OK;
 }
 
+int sqg_max_speed(sqg_plan* pl, const void* u, const void* v, double* out, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!u || !v || !out) return fail(SQG_ERR_INVALID, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  double* part = wsp<double>(pl, pl->off_part);
+  const size_t nn = (size_t)pl->N * pl->N;
+  if (pl->d.precision == SQG_F64)
+    k_speedmax_partial<double><<<kPartBlocks, 256, 0, st>>>((const double*)u, (const double*)v, nn, part);
+  else
+    k_speedmax_partial<float><<<kPartBlocks, 256, 0, st>>>((const float*)u, (const float*)v, nn, part);
+  k_nanmax_final<<<1, 256, 0, st>>>(kPartBlocks, part, out);
+  SQG_CUDA(cudaGetLastError());
+  return SQG_OK;
+}
+
+int sqg_spectrum_absmax(sqg_plan* pl, const void* theta, double* out, void* stream) {
+  int rc = check_ready(pl);
+  if (rc) return rc;
+  if (!theta || !out) return fail(SQG_ERR_INVALID, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  double* part = wsp<double>(pl, pl->off_part);
+  const size_t nn = (size_t)pl->N * pl->N;
+  if (pl->d.precision == SQG_F64)
+    k_cabsmax_partial<double2><<<kPartBlocks, 256, 0, st>>>((const double2*)theta, nn, part);
+  else
+    k_cabsmax_partial<float2><<<kPartBlocks, 256, 0, st>>>((const float2*)theta, nn, part);
+  k_nanmax_final<<<1, 256, 0, st>>>(kPartBlocks, part, out);
+  SQG_CUDA(cudaGetLastError());
+  return SQG_OK;
+}
+
 int sqg_diagnostics(sqg_plan* pl, const void* theta, double* out, void* stream) {
   int rc = check_ready(pl);
   if (rc) return rc;
