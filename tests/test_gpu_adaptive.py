@@ -180,3 +180,24 @@ def test_forced_evolve_fp32():
     fin = res["final_state"]
     assert abs(fin["time"] - 0.05) < 1e-12 and bool(torch.isfinite(torch.view_as_real(fin["theta_hat"])).all())
     assert max(seen) <= 5e-3 and res["statistics"]["n_rejected"] == 0
+
+
+@pytest.mark.parametrize("name", ["rk4_step", "ssp_rk3_step"])
+def test_generic_integrators_on_device_rhs(name):
+    """time_integrator.rk4_step / ssp_rk3_step driven by the library's RHS
+    (solver.compute_rhs) match the float64 oracle's integrators on its RHS."""
+    from oracle import sqg_oracle as O
+    from pygsquig_b200.core import time_integrator as TI
+
+    N, alpha, nu, p, dt = 64, 1.0, 1e-10, 8, 2e-3
+    g = make_grid(N, 2 * math.pi)
+    s = gSQGSolver(g, alpha, nu, p)
+    th = s.initialize(seed=11)["theta_hat"]
+    og = O.make_grid(N, 2 * math.pi)
+    ref = th.cpu().numpy()
+    got = th
+    for _ in range(5):
+        got = getattr(TI, name)(got, s.compute_rhs, dt)
+        ref = getattr(O, name)(ref, lambda t: O.core_rhs(t, og, alpha, nu, p), dt)
+    err = np.linalg.norm(got.cpu().numpy() - ref) / np.linalg.norm(ref)
+    assert err < 1e-12, err
