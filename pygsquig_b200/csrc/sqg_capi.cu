@@ -225,6 +225,10 @@ KP make_kp(const sqg_plan* pl, double dt) {
   kp.tw = pl->ws + pl->off_tw;
   kp.rows = wsp<RowTab>(pl, pl->off_rows);
   kp.inv_n2 = 1.0 / ((double)pl->N * (double)pl->N);
+  {
+    const double dx = d.L / pl->N;  // the expressions of wavenumbers(): same value bit for bit
+    kp.kval = 1.0 / (pl->N * dx);
+  }
   kp.alpha = d.alpha;
   kp.akind = pl->akind;
   kp.scheme = d.scheme;

@@ -49,6 +49,7 @@ struct KP {
   int N, H;
   const double* k1d;  // float64 wavenumbers fftfreq(N, L/N) * 2 pi
   const void* k1t;    // the same in the plan precision
+  double kval;        // 1 / (N dx): fftfreq's scale (the hot kernels compute k from it)
   const void* tw;     // twiddles exp(-2 pi i k/N), plan precision
   const RowTab* rows;
   double inv_n2;      // 1/N^2
@@ -111,6 +112,14 @@ constexpr int min_blocks(int threads) {
 __device__ __forceinline__ int mode_abs(int i, int N) { return i <= (N >> 1) ? i : N - i; }
 
 // |k|^-alpha with k = 0 -> 0 (operators.py:134-155)
+// Wavenumber of index i computed in registers with numpy's operation order
+// for fftfreq(N, L/N) * 2 pi, ((m * val) * 2) * pi, so it equals the k1d table
+// bit for bit without a global load per element.
+__device__ __forceinline__ double wavenumber(const KP& kp, int i) {
+  const int m = i <= ((kp.N - 1) >> 1) ? i : i - kp.N;
+  return __dmul_rn(__dmul_rn(__dmul_rn((double)m, kp.kval), 2.0), 3.141592653589793116);
+}
+
 template <typename T>
 __device__ __forceinline__ T inv_frac(T k2, T alpha, int kind) {
   if (!(k2 > (T)0)) return (T)0;
@@ -171,9 +180,8 @@ __device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, const
                                            typename Cplx<T>::type* wbuf) {
   using C = typename Cplx<T>::type;
   constexpr int N = 1 << LOG2N, G = N / R, H = N / 2, XB = spad_size<R>(N);
-  const T* __restrict__ k1t = reinterpret_cast<const T*>(kp.k1t);
   const C* __restrict__ tw = reinterpret_cast<const C*>(kp.tw);
-  const T kx = k1t[p];
+  const T kx = (T)wavenumber(kp, p);
   const T s_n2 = (T)kp.inv_n2;
   const T dkx = (p == H) ? (T)0 : kx;
   const T nkx = (p == H) ? kx : (T)0;
@@ -184,7 +192,7 @@ __device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, const
     const int iy = j + m * G;
     const C h = cscale(cadd(t1[m], cconj(t2[m])), (T)0.5);
     const C an = cscale(csub(t1[m], cconj(t2[m])), (T)0.5);
-    const T ky = k1t[iy];
+    const T ky = (T)wavenumber(kp, iy);
     const T dky = (iy == H) ? (T)0 : ky;
     const T nky = (iy == H) ? ky : (T)0;
     T mm = (T)0;
@@ -255,10 +263,9 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a) {
   const int pp = (N - p) & (N - 1);
   const bool pair = (p != 0) && (p != H);
   const C* __restrict__ tw = reinterpret_cast<const C*>(kp.tw);
-  const T* __restrict__ k1t = reinterpret_cast<const T*>(kp.k1t);
   const RowTab rt = kp.rows[p];
-  const double kxd = kp.k1d[p];
-  const T kx = k1t[p];
+  const double kxd = wavenumber(kp, p);
+  const T kx = (T)kxd;
   const T s_n2 = (T)kp.inv_n2;
   bool bad = false;
 
@@ -336,7 +343,7 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a) {
       const int my = mode_abs(iy, N);
       cp_async_wait<DEPTH - 1>();  // chunk m has landed (groups are issued in order)
       const C* slot = pf + (size_t)(m % DEPTH) * 4 * G + j;
-      const double kyd = kp.k1d[iy];
+      const double kyd = wavenumber(kp, iy);
       const double k2d = kxd * kxd + kyd * kyd;
       // diagonal linear operator in float64
       double Ld;
