@@ -145,6 +145,12 @@ __device__ __forceinline__ void fft_multi(typename Cplx<T>::type (&v)[NF][R], ty
   constexpr bool INV = DIR > 0;
   static_assert(R == 8 || R == 16, "radix 8 or 16");
   static_assert(LOG2N >= LR, "N >= R");
+  // Twiddle root of the first radix pass, requested before any work: each
+  // pass's root is loaded one pass ahead so the load's latency (the table is
+  // often not L1-resident next to large shared-memory buffers) overlaps the
+  // butterflies and exchange of the pass before.
+  auto root = [&](int pp, int lpp) -> C { return tw[((j & (pp - 1)) << (LOG2N - lpp - LR)) & (N - 1)]; };
+  C w_next = REM != 0 ? root(1 << REM, REM) : C{};
   int p = 1;
   if (REM != 0) {
     constexpr int RP = 1 << REM;
@@ -183,10 +189,12 @@ __device__ __forceinline__ void fft_multi(typename Cplx<T>::type (&v)[NF][R], ty
 #pragma unroll 1
   for (int pass = 0; pass < NPR; ++pass) {
     const int k = j & (p - 1);
+    const C w_cur = w_next;
+    if (pass + 1 < NPR) w_next = root(p * R, lp + LR);
     if (p > 1) {
       // w^r for r = 1..R-1 from one table load w = exp(-+2 pi i k / (p R)):
       // powers by complex products (at most three chained roundings)
-      const C w1 = tw[(k << (LOG2N - lp - LR)) & (N - 1)];
+      const C w1 = w_cur;
       C wp[R];
       wp[1] = w1;
       wp[2] = cmul(w1, w1);
