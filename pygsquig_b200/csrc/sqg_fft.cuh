@@ -21,10 +21,19 @@ template <> struct Cplx<float> { using type = float2; };
 template <> struct Cplx<double> { using type = double2; };
 
 // Shared-memory index of element i in an exchange buffer of a radix-R
-// transform: one padding slot every R elements makes the Stockham store
-// patterns (strides R and R^2 in elements) and the strided loads bank-conflict
-// free.  A padded buffer of N elements occupies spad_size<R>(N) = N + N/R slots.
-template <int R> __device__ __forceinline__ int spad(int i) { return i + (i >> (R == 16 ? 4 : 3)); }
+// transform.  Radix 16, and radix 8 in double precision: one padding slot
+// every R elements.  Radix 8 in single precision: the low four bits of i are
+// XORed with bits 3..9, i ^ (((i >> 3) ^ (i >> 4) ^ (i >> 6)) & 15), which
+// puts the 16 eight-byte accesses of a half-warp in 16 different bank pairs
+// for every pattern of the transform (the strided loads, the stride 1, 8, 64
+// and 512 stores and the radix-2/4 first pass; with the padding rule these
+// took 1.6-1.8 shared-memory wavefronts per ideal one).  It changes only the
+// low four bits, so it permutes each aligned block of 16 elements.  A buffer
+// of N elements occupies spad_size<R>(N) = N + N/R slots.
+template <int R, typename T> __device__ __forceinline__ int spad(int i) {
+  if constexpr (R == 8 && sizeof(T) == 4) return i ^ (((i >> 3) ^ (i >> 4) ^ (i >> 6)) & 15);
+  else return i + (i >> (R == 16 ? 4 : 3));
+}
 template <int R> __host__ __device__ constexpr int spad_size(int n) { return n + n / R; }
 
 template <typename C> __device__ __forceinline__ C mkc(double x, double y) {
@@ -124,7 +133,7 @@ __device__ __forceinline__ void dft16(C (&v)[16]) {
 // NF independent group FFTs executed together.  v[f]: this thread's R
 // values of transform f in strided layout, v[f][m] = x_f[j + m G] with
 // G = N/R (in and out).  sbuf + f * bstride: spad_size<R>(N) complex slots of
-// shared memory for transform f (indexed through spad<R>).  The NF
+// shared memory for transform f (indexed through spad<R, T>).  The NF
 // transforms share every barrier and every twiddle load, which gives each
 // thread NF times the independent work per pass.  All threads of the block
 // must call it together (it uses __syncthreads).  The routine begins with a
@@ -174,13 +183,13 @@ __device__ __forceinline__ void fft_multi(typename Cplx<T>::type (&v)[NF][R], ty
       for (int q = 0; q < NB; ++q) {
         const int i = j + q * G;  // butterfly index, p = 1 so k = 0
 #pragma unroll
-        for (int r = 0; r < RP; ++r) sbuf[f * bstride + spad<R>(i * RP + r)] = v[f][q + r * NB];
+        for (int r = 0; r < RP; ++r) sbuf[f * bstride + spad<R, T>(i * RP + r)] = v[f][q + r * NB];
       }
     __syncthreads();
 #pragma unroll
     for (int f = 0; f < NF; ++f)
 #pragma unroll
-      for (int m = 0; m < R; ++m) v[f][m] = sbuf[f * bstride + spad<R>(j + m * G)];
+      for (int m = 0; m < R; ++m) v[f][m] = sbuf[f * bstride + spad<R, T>(j + m * G)];
     p = RP;
   }
   // Radix-R passes.  The pass loop is kept rolled so that its code is shared
@@ -224,12 +233,12 @@ __device__ __forceinline__ void fft_multi(typename Cplx<T>::type (&v)[NF][R], ty
 #pragma unroll
       for (int f = 0; f < NF; ++f)
 #pragma unroll
-        for (int r = 0; r < R; ++r) sbuf[f * bstride + spad<R>(base + r * p)] = v[f][r];
+        for (int r = 0; r < R; ++r) sbuf[f * bstride + spad<R, T>(base + r * p)] = v[f][r];
       __syncthreads();
 #pragma unroll
       for (int f = 0; f < NF; ++f)
 #pragma unroll
-        for (int m = 0; m < R; ++m) v[f][m] = sbuf[f * bstride + spad<R>(j + m * G)];
+        for (int m = 0; m < R; ++m) v[f][m] = sbuf[f * bstride + spad<R, T>(j + m * G)];
     }
     p *= R;
     lp += LR;

@@ -734,7 +734,7 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
   fft_group<T, LOG2N, R, -1>(W, bufX, j, tw);
   __syncthreads();
 #pragma unroll
-  for (int m = 0; m < R; ++m) bufX[spad<R>(j + m * G)] = W[m];
+  for (int m = 0; m < R; ++m) bufX[spad<R, T>(j + m * G)] = W[m];
   __syncthreads();
   // split: Ja(kx) = (W(kx) + conj W(-kx))/2, Jb(kx) = -i (W(kx) - conj W(-kx))/2
   C* jh = reinterpret_cast<C*>(a.jh);
@@ -743,8 +743,8 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
     const int kx = idx / np;
     const int q = idx - kx * np;
     const C* w = smem + (size_t)q * NBUF * SZ;
-    const C wk = w[spad<R>(kx)];
-    const C wm = w[spad<R>((N - kx) & (N - 1))];
+    const C wk = w[spad<R, T>(kx)];
+    const C wm = w[spad<R, T>((N - kx) & (N - 1))];
     const C ja = mkc<C>((T)0.5 * (wk.x + wm.x), (T)0.5 * (wk.y - wm.y));
     const C d = mkc<C>(wk.x - wm.x, wk.y + wm.y);
     const C jb = mkc<C>((T)0.5 * d.y, (T)-0.5 * d.x);
