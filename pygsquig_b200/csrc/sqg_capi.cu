@@ -320,8 +320,9 @@ constexpr int row_depth() {
 template <typename T, int L>
 size_t row_smem() { return row_base_smem<T, L>() + row_pf_bytes<T, L>(row_depth<T, L>()); }
 template <typename T, int L>
-size_t col_smem() {
-  return (size_t)pairs_per_cta<T, L>() * col_nbuf<T, L>() * ColBuf<(1 << L), col_radix<T, L>()>::SZ *
+size_t col_smem() {  // per column pair: NBUF buffers plus the slack of col_qstride
+  return (size_t)pairs_per_cta<T, L>() *
+         (col_nbuf<T, L>() * ColBuf<(1 << L), col_radix<T, L>()>::SZ + line_elems<T>()) *
          sizeof(typename Cplx<T>::type);
 }
 

@@ -538,9 +538,32 @@ struct ColArgs {
 };
 
 // Slots of one field buffer of a column group: the raw half columns
-// A[kx] = x(kx, ya) at slot kx and B[kx] = x(kx, ya + 1) at slot H + 1 + kx
-// (kx = 0..N/2), later reused as the padded FFT exchange buffer.
+// A[kx] = x(kx, ya) at slot kx and B[kx] = x(kx, ya + 1) at slot
+// col_offb + kx (kx = 0..N/2), later reused as the FFT exchange buffer.
 template <int N, int R> struct ColBuf { static constexpr int SZ = spad_size<R>(N) + 2; };
+
+// Placement of the raw half columns, chosen for the cp.async writes of
+// col_fetch: consecutive threads write (column pair q, half b, row kx) with
+// (q, b) fastest, so the 16 eight-byte writes of a half-warp (8 sixteen-byte
+// writes of a quarter-warp in double) span 2 np groups of rows.  B starts L/2
+// slots past a multiple of the line (L = elements per 128-byte line) and the
+// buffers of pair q start q * col_qstride(np), with col_qstride = L / (2 np)
+// modulo L, so the groups fill distinct banks (placed at H + 1 and
+// q * NBUF * SZ they took two to four shared-memory wavefronts per ideal one).
+// Each pair's buffers carry L slack slots for the stride adjustment.
+template <typename T> __host__ __device__ constexpr int line_elems() {
+  return 128 / (int)sizeof(typename Cplx<T>::type);
+}
+template <typename T, int N, int R> __host__ __device__ constexpr int col_offb() {
+  constexpr int L = line_elems<T>(), H = N / 2;
+  constexpr int off = H + 1 + ((L / 2 - (H + 1)) % L + L) % L;
+  return off + H + 1 <= ColBuf<N, R>::SZ ? off : H + 1;
+}
+template <typename T, int N, int R, int NBUF> __device__ __forceinline__ int col_qstride(int np) {
+  constexpr int L = line_elems<T>(), base = NBUF * ColBuf<N, R>::SZ;
+  const int want = 2 * np <= L ? L / (2 * np) : 1;
+  return base + ((want - base) % L + L) % L;
+}
 
 // Issue the copies of the half columns of field f for every column pair of
 // the block into buffer slot `buf` of each group (no registers, no wait).
@@ -548,14 +571,15 @@ template <typename T, int LOG2N, int R, int NP, int NBUF>
 __device__ __forceinline__ void col_fetch(const typename Cplx<T>::type* __restrict__ f, int y0, int buf,
                                           typename Cplx<T>::type* smem, int np) {
   using C = typename Cplx<T>::type;
-  constexpr int N = 1 << LOG2N, H = N / 2, SZ = ColBuf<N, R>::SZ;
+  constexpr int N = 1 << LOG2N, H = N / 2, SZ = ColBuf<N, R>::SZ, OFFB = col_offb<T, N, R>();
+  const int qs = col_qstride<T, N, R, NBUF>(np);
   const int total = (H + 1) * np * 2;
   for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
     const int c = idx % (2 * np);      // column within the block (fastest: coalesced rows)
     const int kx = idx / (2 * np);
     const int q = c >> 1, b = c & 1;
-    C* z = smem + (size_t)(q * NBUF + buf) * SZ;
-    cp_async_elem(z + b * (H + 1) + kx, f + (size_t)kx * N + y0 + c, (int)sizeof(C));
+    C* z = smem + (size_t)q * qs + (size_t)buf * SZ;
+    cp_async_elem(z + b * OFFB + kx, f + (size_t)kx * N + y0 + c, (int)sizeof(C));
   }
 }
 
@@ -565,12 +589,12 @@ template <typename T, int LOG2N, int R>
 __device__ __forceinline__ void col_first_load(const typename Cplx<T>::type* z, int j,
                                                typename Cplx<T>::type (&v)[R]) {
   using C = typename Cplx<T>::type;
-  constexpr int N = 1 << LOG2N, H = N / 2, G = N / R;
+  constexpr int N = 1 << LOG2N, H = N / 2, G = N / R, OFFB = col_offb<T, N, R>();
 #pragma unroll
   for (int m = 0; m < R; ++m) {
     const int x = j + m * G;
     const int kx = x <= H ? x : N - x;
-    const C xa = z[kx], xb = z[H + 1 + kx];
+    const C xa = z[kx], xb = z[OFFB + kx];
     if (x == 0 || x == H) v[m] = mkc<C>(xa.x, xb.x);
     else if (x < H) v[m] = mkc<C>(xa.x - xb.y, xa.y + xb.x);
     else v[m] = mkc<C>(xa.x + xb.y, -xa.y + xb.x);
@@ -598,8 +622,9 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
   }
   const int grp = threadIdx.x / G;
   const int j = threadIdx.x - grp * G;
-  C* gbuf = smem + (size_t)grp * NBUF * SZ;  // this group's NBUF buffers
   const int np = a.np > 0 ? a.np : NP;       // launch shape (autotuned), <= NP
+  const int qs = col_qstride<T, N, R, NBUF>(np);
+  C* gbuf = smem + (size_t)grp * qs;         // this group's NBUF buffers
   const int y0 = blockIdx.x * (2 * np);
   const int ya = y0 + 2 * grp;
   const C* __restrict__ tw = reinterpret_cast<const C*>(kp.tw);
@@ -742,7 +767,7 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
   for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
     const int kx = idx / np;
     const int q = idx - kx * np;
-    const C* w = smem + (size_t)q * NBUF * SZ;
+    const C* w = smem + (size_t)q * qs;
     const C wk = w[spad<R, T>(kx)];
     const C wm = w[spad<R, T>((N - kx) & (N - 1))];
     const C ja = mkc<C>((T)0.5 * (wk.x + wm.x), (T)0.5 * (wk.y - wm.y));
