@@ -331,23 +331,39 @@ size_t col_smem() {  // per column pair: NBUF buffers plus the slack of col_qstr
 // shared memory scales with it.  Results do not depend on the shape (every
 // row and column transform is computed the same way); only the number and
 // size of the CTAs change.
+// The row and column passes are launched with programmatic stream
+// serialisation (see pdl_enter in sqg_kernels.cuh): the next pass's launch and
+// block scheduling overlap the tail of the current one.
+template <typename Arg>
+cudaError_t launch_pdl(void (*kernel)(KP, Arg), int grid, int block, size_t smem, cudaStream_t st, const KP& kp,
+                       const Arg& a) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, kp, a);
+}
 template <typename T, int L>
 cudaError_t launch_row_t(const KP& kp, const RowArgs& a, cudaStream_t st) {
   constexpr int N = 1 << L, RPC = rows_per_cta<T, L>();
   const int rpc = a.rpc > 0 ? a.rpc : RPC;
   const int grid = (N / 2 + 1 + rpc - 1) / rpc;
-  k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>
-      <<<grid, rpc * row_group<T, L>(), row_smem<T, L>() / RPC * rpc, st>>>(kp, a);
-  return cudaGetLastError();
+  return launch_pdl(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>, grid,
+                    rpc * row_group<T, L>(), row_smem<T, L>() / RPC * rpc, st, kp, a);
 }
 template <typename T, int L>
 cudaError_t launch_col_t(const KP& kp, const ColArgs& a, cudaStream_t st, bool ring_only) {
   constexpr int N = 1 << L, NP = pairs_per_cta<T, L>();
   const int np = a.np > 0 ? a.np : NP;
   int grid = ring_only ? 1 : N / (2 * np) + (a.ring_cta ? 1 : 0);
-  k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()>
-      <<<grid, np * col_group<T, L>(), col_smem<T, L>() / NP * np, st>>>(kp, a);
-  return cudaGetLastError();
+  return launch_pdl(k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()>, grid, np * col_group<T, L>(),
+                    col_smem<T, L>() / NP * np, st, kp, a);
 }
 template <typename T, int L>
 cudaError_t shape_max_t(int* rpc, int* np) {
