@@ -23,9 +23,9 @@ CSRC = os.path.join(HERE, "csrc")
 SRCS = [os.path.join(CSRC, f) for f in ("sqg_capi.cu", "closure_conv.cu", "closure_ops.cu")]
 # headers each unit includes (a change rebuilds the unit)
 DEPS = {
-    "sqg_capi.cu": ["sqg_fft.cuh", "sqg_kernels.cuh", "sqg_aux.cuh", "../../include/sqg.h"],
-    "closure_conv.cu": ["closure_act.cuh", "../../include/sqg_closure.h"],
-    "closure_ops.cu": ["closure_act.cuh", "../../include/sqg_closure.h"],
+    "sqg_capi.cu": ["pdl.cuh", "sqg_fft.cuh", "sqg_kernels.cuh", "sqg_aux.cuh", "../../include/sqg.h"],
+    "closure_conv.cu": ["pdl.cuh", "closure_act.cuh", "../../include/sqg_closure.h"],
+    "closure_ops.cu": ["pdl.cuh", "closure_act.cuh", "../../include/sqg_closure.h"],
 }
 OUT = os.path.join(HERE, "libsqg.so")
 OBJ_DIR = os.path.join(HERE, "_build")

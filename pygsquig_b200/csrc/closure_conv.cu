@@ -44,6 +44,7 @@
 
 #include "../../include/sqg_closure.h"
 #include "closure_act.cuh"
+#include "pdl.cuh"
 
 namespace {
 
@@ -200,6 +201,7 @@ __device__ __forceinline__ uint32_t sw128_off(int r, int c) { return (uint32_t)r
 __global__ void __launch_bounds__(kThreads, 1)
 k_conv64(const __grid_constant__ CUtensorMap act_map, const __grid_constant__ CUtensorMap w_map,
          const __grid_constant__ CUtensorMap out_map, const __grid_constant__ CUtensorMap z_map, ConvArgs a) {
+  pdl_wait();  // the previous kernel's output (this layer's input) is visible after this
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte aligned carve-up
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -638,8 +640,8 @@ int closure_conv64(int32_t B, int32_t H, int32_t W, int32_t mode, const void* ac
   const int n_tiles = B * H * (W / kTileM);
   int g = grid > 0 ? grid : 148;
   if (g > n_tiles) g = n_tiles;
-  k_conv64<<<g, kThreads, kSmemBytes, (cudaStream_t)stream>>>(amap, wmap, omap, zmap, a);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launch_pdl(k_conv64, dim3(g), dim3(kThreads), kSmemBytes, (cudaStream_t)stream, amap, wmap, omap,
+                             zmap, a);
   if (e != cudaSuccess) return cfail(2, std::string("closure_conv64 launch: ") + cudaGetErrorString(e));
   return 0;
 }

@@ -14,6 +14,7 @@
 
 #include "../../include/sqg_closure.h"
 #include "closure_act.cuh"
+#include "pdl.cuh"
 
 namespace {
 
@@ -123,6 +124,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_conv_in(int B, int H, int W, fl
                                                          const float* __restrict__ w, const float* __restrict__ bias,
                                                          __nv_bfloat16* __restrict__ z, __nv_bfloat16* __restrict__ a_pad) {
   __shared__ float stg[kWarps][3][34];
+  pdl_wait();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane >> 3, g = lane & 7;
   float wr[9][8], b8[8];
@@ -169,6 +171,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_conv_out(int B, int H, int W, f
                                                           const __nv_bfloat16* __restrict__ a_pad,
                                                           const float* __restrict__ w, const float* __restrict__ bias,
                                                           float* __restrict__ y) {
+  pdl_wait();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float w0[9], w1[9];
 #pragma unroll
@@ -382,18 +385,18 @@ int closure_conv_in(int32_t B, int32_t H, int32_t W, float in_scale, const float
                     void* z, void* a_pad, void* stream) {
   if (!x || !w || !bias || !z || !a_pad) return ofail("closure_conv_in: null pointer");
   if (!shape_ok(B, H, W)) return ofail("closure_conv_in: need B >= 1, H >= 2 and W a positive multiple of 32");
-  k_conv_in<<<grid_for(B, H, W), kWarps * 32, 0, (cudaStream_t)stream>>>(B, H, W, in_scale, x, w, bias,
-                                                                         (__nv_bfloat16*)z, (__nv_bfloat16*)a_pad);
-  return cudaGetLastError() == cudaSuccess ? 0 : ofail("closure_conv_in: launch failed");
+  const cudaError_t e = launch_pdl(k_conv_in, grid_for(B, H, W), dim3(kWarps * 32), 0, (cudaStream_t)stream, B, H, W,
+                                   in_scale, x, w, bias, (__nv_bfloat16*)z, (__nv_bfloat16*)a_pad);
+  return e == cudaSuccess ? 0 : ofail("closure_conv_in: launch failed");
 }
 
 int closure_conv_out(int32_t B, int32_t H, int32_t W, float out_scale, const void* a_pad, const float* w,
                      const float* bias, float* y, void* stream) {
   if (!a_pad || !w || !bias || !y) return ofail("closure_conv_out: null pointer");
   if (!shape_ok(B, H, W)) return ofail("closure_conv_out: need B >= 1, H >= 2 and W a positive multiple of 32");
-  k_conv_out<<<grid_for(B, H, W), kWarps * 32, 0, (cudaStream_t)stream>>>(B, H, W, out_scale,
-                                                                          (const __nv_bfloat16*)a_pad, w, bias, y);
-  return cudaGetLastError() == cudaSuccess ? 0 : ofail("closure_conv_out: launch failed");
+  const cudaError_t e = launch_pdl(k_conv_out, grid_for(B, H, W), dim3(kWarps * 32), 0, (cudaStream_t)stream, B, H, W,
+                                   out_scale, (const __nv_bfloat16*)a_pad, w, bias, y);
+  return e == cudaSuccess ? 0 : ofail("closure_conv_out: launch failed");
 }
 
 int closure_conv_out_dgrad(int32_t B, int32_t H, int32_t W, const float* gy, const float* w, const void* z,

@@ -257,6 +257,7 @@ __global__ void __launch_bounds__(256) k_ring_substeps(int N, int n, const int* 
                                                        double amp, double eps, int n_sub, double dt,
                                                        const double* __restrict__ phases,
                                                        typename Cplx<T>::type* theta, double2* F) {
+  pdl_wait();
   using C = typename Cplx<T>::type;
   constexpr int V = 256;
   __shared__ double red_r[V], red_q[V];

@@ -331,38 +331,22 @@ size_t col_smem() {  // per column pair: NBUF buffers plus the slack of col_qstr
 // shared memory scales with it.  Results do not depend on the shape (every
 // row and column transform is computed the same way); only the number and
 // size of the CTAs change.
-// The row and column passes are launched with programmatic stream
-// serialisation (see pdl_enter in sqg_kernels.cuh): the next pass's launch and
-// block scheduling overlap the tail of the current one.
-template <typename Arg>
-cudaError_t launch_pdl(void (*kernel)(KP, Arg), int grid, int block, size_t smem, cudaStream_t st, const KP& kp,
-                       const Arg& a) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(block);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kernel, kp, a);
-}
+// The row and column passes are launched with programmatic dependent launch
+// (pdl.cuh): the next pass's launch overlaps the tail of the current one.
 template <typename T, int L>
 cudaError_t launch_row_t(const KP& kp, const RowArgs& a, cudaStream_t st) {
   constexpr int N = 1 << L, RPC = rows_per_cta<T, L>();
   const int rpc = a.rpc > 0 ? a.rpc : RPC;
   const int grid = (N / 2 + 1 + rpc - 1) / rpc;
-  return launch_pdl(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>, grid,
-                    rpc * row_group<T, L>(), row_smem<T, L>() / RPC * rpc, st, kp, a);
+  return launch_pdl(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>, dim3(grid),
+                    dim3(rpc * row_group<T, L>()), row_smem<T, L>() / RPC * rpc, st, kp, a);
 }
 template <typename T, int L>
 cudaError_t launch_col_t(const KP& kp, const ColArgs& a, cudaStream_t st, bool ring_only) {
   constexpr int N = 1 << L, NP = pairs_per_cta<T, L>();
   const int np = a.np > 0 ? a.np : NP;
   int grid = ring_only ? 1 : N / (2 * np) + (a.ring_cta ? 1 : 0);
-  return launch_pdl(k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()>, grid, np * col_group<T, L>(),
+  return launch_pdl(k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()>, dim3(grid), dim3(np * col_group<T, L>()),
                     col_smem<T, L>() / NP * np, st, kp, a);
 }
 template <typename T, int L>
@@ -1060,12 +1044,11 @@ int sqg_ring_substeps(sqg_plan* pl, void* theta, int32_t n_sub, double dt_sub, c
   const int* pos = wsp<int>(pl, pl->off_ring_pos);
   const int* mir = wsp<int>(pl, pl->off_ring_mirror);
   if (pl->d.precision == SQG_F64)
-    k_ring_substeps<double><<<1, 256, 0, st>>>(pl->N, n, pos, mir, ho, pl->d.ring_amplitude, pl->d.ring_epsilon, n_sub,
-                                               dt_sub, phases, (double2*)theta, F);
+    SQG_CUDA(launch_pdl(k_ring_substeps<double>, dim3(1), dim3(256), 0, st, pl->N, n, pos, mir, ho,
+                        pl->d.ring_amplitude, pl->d.ring_epsilon, n_sub, dt_sub, phases, (double2*)theta, F));
   else
-    k_ring_substeps<float><<<1, 256, 0, st>>>(pl->N, n, pos, mir, ho, pl->d.ring_amplitude, pl->d.ring_epsilon, n_sub,
-                                              dt_sub, phases, (float2*)theta, F);
-  SQG_CUDA(cudaGetLastError());
+    SQG_CUDA(launch_pdl(k_ring_substeps<float>, dim3(1), dim3(256), 0, st, pl->N, n, pos, mir, ho,
+                        pl->d.ring_amplitude, pl->d.ring_epsilon, n_sub, dt_sub, phases, (float2*)theta, F));
   pl->launches++;
   return SQG_OK;
 }
@@ -1473,17 +1456,15 @@ template <typename T, int L>
 cudaError_t launch_row_batch_t(const KP* kps, const RowArgs* as, int members, cudaStream_t st) {
   constexpr int N = 1 << L, RPC = rows_per_cta<T, L>();
   dim3 grid((N / 2 + 1 + RPC - 1) / RPC, members);
-  k_row_batch<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>
-      <<<grid, RPC * row_group<T, L>(), row_smem<T, L>(), st>>>(kps, as);
-  return cudaGetLastError();
+  return launch_pdl(k_row_batch<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>, grid,
+                    dim3(RPC * row_group<T, L>()), row_smem<T, L>(), st, kps, as);
 }
 template <typename T, int L>
 cudaError_t launch_col_batch_t(const KP* kps, const ColArgs* as, int members, cudaStream_t st) {
   constexpr int N = 1 << L, NP = pairs_per_cta<T, L>();
   dim3 grid(N / (2 * NP), members);
-  k_col_batch<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()>
-      <<<grid, NP * col_group<T, L>(), col_smem<T, L>(), st>>>(kps, as);
-  return cudaGetLastError();
+  return launch_pdl(k_col_batch<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()>, grid,
+                    dim3(NP * col_group<T, L>()), col_smem<T, L>(), st, kps, as);
 }
 template <typename T, int L>
 cudaError_t set_batch_attrs_t() {

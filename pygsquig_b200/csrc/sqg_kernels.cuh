@@ -24,6 +24,7 @@
 // (k, -k) reproduces the reference exactly, including at the Nyquist row and
 // column where a derivative multiplier is not Hermitian-symmetric.
 #pragma once
+#include "pdl.cuh"
 #include "sqg_fft.cuh"
 
 namespace sqg {
@@ -868,28 +869,18 @@ __global__ void k_set_ctl(RingCtl* ctl, const double* base) {
 }  // namespace sqg
 
 namespace sqg {
-// Programmatic dependent launch.  The passes are launched with programmatic
-// stream serialisation, so the next pass's launch begins as the blocks of the
-// current one exit instead of after the grid's completion has been
-// processed; every block first waits until the previous grid has completed
-// and its writes are visible (griddepcontrol.wait; a no-op when the launch
-// had no programmatic dependency).  No global memory is touched before the
-// wait.  (Allowing the dependents to launch at a block's start was slower at
-// N = 4096.)
-__device__ __forceinline__ void pdl_enter() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
-
 // ---- kernels: one plan, or a batch of members (member = blockIdx.y) ----
 template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
 __global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), min_blocks<T>(RPC * ((1 << LOG2N) / R)))
 k_row(KP kp, RowArgs a) {
-  pdl_enter();
+  pdl_wait();
   row_body<T, LOG2N, R, RPC, DEPTH, NFX>(kp, a);
 }
 
 template <typename T, int LOG2N, int R, int NP, int NBUF>
 __global__ void __launch_bounds__(NP * ((1 << LOG2N) / R), min_blocks<T>(NP * ((1 << LOG2N) / R)))
 k_col(KP kp, ColArgs a) {
-  pdl_enter();
+  pdl_wait();
   col_body<T, LOG2N, R, NP, NBUF>(kp, a);
 }
 
@@ -898,6 +889,7 @@ k_col(KP kp, ColArgs a) {
 template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
 __global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), min_blocks<T>(RPC * ((1 << LOG2N) / R)))
 k_row_batch(const KP* __restrict__ kps, const RowArgs* __restrict__ as) {
+  pdl_wait();
   const KP kp = kps[blockIdx.y];
   const RowArgs a = as[blockIdx.y];
   if (a.xh == nullptr && a.rhs_out == nullptr) return;
@@ -907,6 +899,7 @@ k_row_batch(const KP* __restrict__ kps, const RowArgs* __restrict__ as) {
 template <typename T, int LOG2N, int R, int NP, int NBUF>
 __global__ void __launch_bounds__(NP * ((1 << LOG2N) / R), min_blocks<T>(NP * ((1 << LOG2N) / R)))
 k_col_batch(const KP* __restrict__ kps, const ColArgs* __restrict__ as) {
+  pdl_wait();
   const KP kp = kps[blockIdx.y];
   const ColArgs a = as[blockIdx.y];
   if (a.xh == nullptr) return;
