@@ -334,5 +334,14 @@ def get_plan(key: PlanKey) -> Plan:
     return pl
 
 
+_GENERATION = [0]
+
+
+def plan_generation() -> int:
+    """Incremented by clear_plans (callers that keep plans drop them then)."""
+    return _GENERATION[0]
+
+
 def clear_plans() -> None:
     _CACHE.clear()
+    _GENERATION[0] += 1

@@ -31,7 +31,7 @@ from typing import Callable, Optional
 import numpy as np
 import torch
 
-from .._plan import Plan, PlanKey, get_plan
+from .._plan import Plan, PlanKey, get_plan, plan_generation
 from ..exceptions import NumericalError
 from .. import _lib
 from ..forcing.damping import CombinedDamping
@@ -76,13 +76,29 @@ class gSQGSolver:
             scalars=self._scalar_tuples(), role=role,
         )
 
+    def _cached_plan(self, damping, ring, role) -> Plan:
+        # The plan cache keyed by PlanKey costs a dataclass construction and
+        # hash per call; this per-solver lookup on plain tuples is what a step
+        # pays on the host.  The key holds every input of plan_key.
+        k = (plan_generation(), role, self.alpha, self.nu_p, self.p, self.precision, self.scheme,
+             self._scalar_tuples(), None if damping is None else damping.plan_tuple(),
+             None if ring is None else ring.plan_tuple(),
+             torch.cuda.current_device() if torch.cuda.is_available() else -1)
+        cache = self.__dict__.setdefault("_plans", {})
+        pl = cache.get(k)
+        if pl is None:
+            if len(cache) > 32:
+                cache.clear()
+            pl = cache[k] = get_plan(self.plan_key(damping, ring, role=role))
+        return pl
+
     def plan(self, damping=None, ring=None) -> Plan:
-        return get_plan(self.plan_key(damping, ring))
+        return self._cached_plan(damping, ring, "step")
 
     def aux_plan(self) -> Plan:
         """Plan for transforms, velocity, RHS and diagnostics: its own
         workspace, so a forcing callable may use them between RK stages."""
-        return get_plan(self.plan_key(role="aux"))
+        return self._cached_plan(None, None, "aux")
 
     @property
     def cdtype(self):
