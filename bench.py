@@ -84,7 +84,7 @@ def ensemble_members(O, seed=7):
 
 
 def bytes_per_launch(N, w_bytes):
-    """Algorithmic bytes of each pass per launch (model stated in DESIGN.md).
+    """Algorithmic bytes of each pass per launch.
 
     P = N^2, half array = (N/2+1) N complex = ~w P bytes, full spectrum = 2 w P.
     column pass: reads 4 half arrays, writes 1 half array.
@@ -518,7 +518,7 @@ def main():
     dom = max((k for k in kern if "achieved_gbs" in kern[k]), key=lambda k: kern[k]["share"])
     value = world * main_res["steps"] / (main_res["ms"] / 1e3)
     ms_per_step = main_res["ms"] / main_res["steps"]
-    model_bytes = 88 * wb * N * N  # SURVEY model: 88 w N^2 per RK4 step
+    model_bytes = 88 * wb * N * N  # step model: 88 w N^2 bytes per RK4 step
     line = {
         "metric": "RK4 steps/s", "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",

@@ -1,6 +1,6 @@
 """CPU float64 oracle for the pygSQuiG right-hand-side and RK4 hot path.
 
-TEST INFRASTRUCTURE ONLY.  This module is the checker: only ``tests/``,
+TEST INFRASTRUCTURE ONLY.  It checks the CUDA path: only ``tests/``,
 ``__graft_entry__.smoke()`` and the CPU-baseline legs of ``bench.py`` may
 import it.  The product path (``pygsquig_b200``) never calls it and fails
 loudly when its CUDA library is missing.
