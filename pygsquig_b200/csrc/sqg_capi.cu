@@ -254,7 +254,7 @@ KP make_kp(const sqg_plan* pl, double dt) {
 template <typename T, int L>
 constexpr int col_radix() { return (sizeof(T) == 4 && L >= 11) ? 16 : 8; }
 template <typename T, int L>
-constexpr int row_radix() { return 8; }
+constexpr int row_radix() { return (sizeof(T) == 4 && L >= 7 && L <= 10) ? 4 : 8; }
 template <typename T, int L>
 constexpr int row_group() { return (1 << L) / row_radix<T, L>(); }
 template <typename T, int L>
@@ -282,7 +282,7 @@ constexpr int col_nbuf() {
 // radix-16 row pass.
 template <typename T, int L>
 constexpr int row_nfx() {
-  return row_radix<T, L>() == 16 ? 2
+  return row_radix<T, L>() != 8 ? 2
          : (size_t)rows_per_cta<T, L>() * 4 * spad_size<row_radix<T, L>()>(1 << L) * sizeof(typename Cplx<T>::type) <=
                    150 * 1024 ? 4 : 2;
 }
@@ -301,7 +301,7 @@ constexpr size_t row_pf_bytes(int depth) {
 // per block), the deepest among equals: occupancy first, then prefetch depth.
 template <typename T, int L>
 constexpr int row_occupancy(int depth) {
-  constexpr int by_regs = min_blocks<T>(rows_per_cta<T, L>() * row_group<T, L>());
+  constexpr int by_regs = row_min_blocks<T, row_radix<T, L>()>(rows_per_cta<T, L>() * row_group<T, L>());
   const size_t smem = row_base_smem<T, L>() + row_pf_bytes<T, L>(depth);
   if (smem > 220 * 1024) return 0;
   const int by_smem = (int)((227 * 1024) / (smem + 1024));

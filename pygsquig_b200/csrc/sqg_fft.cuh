@@ -28,10 +28,13 @@ template <> struct Cplx<double> { using type = double2; };
 // for every pattern of the transform (the strided loads, the stride 1, 8, 64
 // and 512 stores and the radix-2/4 first pass; with the padding rule these
 // took 1.6-1.8 shared-memory wavefronts per ideal one).  It changes only the
-// low four bits, so it permutes each aligned block of 16 elements.  A buffer
-// of N elements occupies spad_size<R>(N) = N + N/R slots.
+// low four bits, so it permutes each aligned block of 16 elements.  Radix 4
+// in single precision: i ^ ((i >> 2) & 15), conflict-free for its patterns in
+// the same way.  A buffer of N elements occupies spad_size<R>(N) = N + N/R
+// slots.
 template <int R, typename T> __device__ __forceinline__ int spad(int i) {
   if constexpr (R == 8 && sizeof(T) == 4) return i ^ (((i >> 3) ^ (i >> 4) ^ (i >> 6)) & 15);
+  else if constexpr (R == 4 && sizeof(T) == 4) return i ^ ((i >> 2) & 15);
   else return i + (i >> (R == 16 ? 4 : 3));
 }
 template <int R> __host__ __device__ constexpr int spad_size(int n) { return n + n / R; }
@@ -146,13 +149,13 @@ template <typename T, int LOG2N, int R, int DIR, int NF>
 __device__ __forceinline__ void fft_multi(typename Cplx<T>::type (&v)[NF][R], typename Cplx<T>::type* sbuf,
                                           int bstride, int j, const typename Cplx<T>::type* __restrict__ tw) {
   using C = typename Cplx<T>::type;
-  constexpr int LR = R == 16 ? 4 : 3;
+  constexpr int LR = R == 16 ? 4 : (R == 8 ? 3 : 2);
   constexpr int N = 1 << LOG2N;
   constexpr int G = N / R;
   constexpr int REM = LOG2N % LR;
   constexpr int NPR = LOG2N / LR;
   constexpr bool INV = DIR > 0;
-  static_assert(R == 8 || R == 16, "radix 8 or 16");
+  static_assert(R == 4 || R == 8 || R == 16, "radix 4, 8 or 16");
   static_assert(LOG2N >= LR, "N >= R");
   // Twiddle root of the first radix pass, requested before any work: each
   // pass's root is loaded one pass ahead so the load's latency (the table is
@@ -168,9 +171,9 @@ __device__ __forceinline__ void fft_multi(typename Cplx<T>::type (&v)[NF][R], ty
     for (int f = 0; f < NF; ++f)
 #pragma unroll
       for (int q = 0; q < NB; ++q) {
-        if (RP == 2) {
+        if constexpr (RP == 2) {
           dft2<DIR>(v[f][q], v[f][q + NB]);
-        } else if (RP == 4) {
+        } else if constexpr (RP == 4) {
           dft4<DIR>(v[f][q], v[f][q + NB], v[f][q + 2 * NB], v[f][q + 3 * NB]);
         } else {
           dft8s<DIR, T>(v[f], q, NB);
@@ -208,10 +211,12 @@ __device__ __forceinline__ void fft_multi(typename Cplx<T>::type (&v)[NF][R], ty
       wp[1] = w1;
       wp[2] = cmul(w1, w1);
       wp[3] = cmul(wp[2], w1);
-      wp[4] = cmul(wp[2], wp[2]);
-      wp[5] = cmul(wp[4], w1);
-      wp[6] = cmul(wp[3], wp[3]);
-      wp[7] = cmul(wp[4], wp[3]);
+      if constexpr (R >= 8) {
+        wp[4] = cmul(wp[2], wp[2]);
+        wp[5] = cmul(wp[4], w1);
+        wp[6] = cmul(wp[3], wp[3]);
+        wp[7] = cmul(wp[4], wp[3]);
+      }
       if constexpr (R == 16) {
         wp[8] = cmul(wp[4], wp[4]);
 #pragma unroll
@@ -225,7 +230,8 @@ __device__ __forceinline__ void fft_multi(typename Cplx<T>::type (&v)[NF][R], ty
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
       if constexpr (R == 16) dft16<DIR, T>(v[f]);
-      else dft8s<DIR, T>(v[f], 0, 1);
+      else if constexpr (R == 8) dft8s<DIR, T>(v[f], 0, 1);
+      else dft4<DIR>(v[f][0], v[f][1], v[f][2], v[f][3]);
     }
     if (pass != NPR - 1) {
       __syncthreads();

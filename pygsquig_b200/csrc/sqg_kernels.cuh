@@ -109,6 +109,13 @@ constexpr int min_blocks(int threads) {
   return sizeof(T) == 4 ? (65536 / (threads * 128) > 8 ? 8 : (65536 / (threads * 128) > 0 ? 65536 / (threads * 128) : 1))
                         : (65536 / (threads * 168) > 8 ? 8 : (65536 / (threads * 168) > 0 ? 65536 / (threads * 168) : 1));
 }
+// Row pass: radix 4 (single precision, N <= 1024) keeps few values per thread,
+// so its blocks are held to 64 registers a thread (twice the resident warps).
+template <typename T, int R>
+constexpr int row_min_blocks(int threads) {
+  return (R == 4 && sizeof(T) == 4) ? (65536 / (threads * 64) > 8 ? 8 : (65536 / (threads * 64) > 0 ? 65536 / (threads * 64) : 1))
+                                    : min_blocks<T>(threads);
+}
 
 __device__ __forceinline__ int mode_abs(int i, int N) { return i <= (N >> 1) ? i : N - i; }
 
@@ -871,7 +878,7 @@ __global__ void k_set_ctl(RingCtl* ctl, const double* base) {
 namespace sqg {
 // ---- kernels: one plan, or a batch of members (member = blockIdx.y) ----
 template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
-__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), min_blocks<T>(RPC * ((1 << LOG2N) / R)))
+__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), row_min_blocks<T, R>(RPC * ((1 << LOG2N) / R)))
 k_row(KP kp, RowArgs a) {
   pdl_wait();
   row_body<T, LOG2N, R, RPC, DEPTH, NFX>(kp, a);
@@ -887,7 +894,7 @@ k_col(KP kp, ColArgs a) {
 // Batched forms: the member's parameters come from device arrays; members
 // with no work in this pass have a null xh pointer and return at once.
 template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
-__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), min_blocks<T>(RPC * ((1 << LOG2N) / R)))
+__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), row_min_blocks<T, R>(RPC * ((1 << LOG2N) / R)))
 k_row_batch(const KP* __restrict__ kps, const RowArgs* __restrict__ as) {
   pdl_wait();
   const KP kp = kps[blockIdx.y];

@@ -272,6 +272,29 @@ def test_fp32_error_vs_fp64_oracle(P):
     assert err < 2e-5
 
 
+@pytest.mark.parametrize("N", [128, 256, 512, 1024])
+def test_fp32_forced_ifrk4_vs_fp64_oracle(P, N):
+    """FP32 forced, damped IF-RK4 (the sizes whose row pass is radix 4, incl.
+    the radix-2 first pass at N = 128 and 512) against the float64 oracle
+    restatement: relative L2 < 2e-5 after 4 steps (FP32 transform round-off)."""
+    dt, kf = 2e-4, N / 16
+    go = O.make_grid(N, TWO_PI)
+    rng = np.random.default_rng(N)
+    th0 = O.random_phase_field(go, lambda k: k**4 * np.exp(-((k / (N / 64)) ** 2)), 3)
+    ring_o = O.RingForcing(kf, 2.0, 0.1)
+    damp_o = O.CombinedDamping(0.1, kf, 1e-8 * (1024 / N) ** 8, 8)
+    so = O.gSQGSolver(go, 1.0, 0.0, 8, scheme="ifrk4")
+    phases = rng.uniform(0, 2 * np.pi, size=(4, O.ring_mode_count(go, kf, 2.0)))
+    sto = so.initialize(theta0=th0)
+    for i in range(4):
+        sto = O.step_forced(so, sto, dt, ring_o, phases[i], damp_o)
+    s = P.gSQGSolver(P.make_grid(N, TWO_PI), 1.0, 0.0, 8, precision="float32", scheme="ifrk4")
+    st = s.multistep(s.initialize(theta0=th0), 4, dt, forcing=P.RingForcing(kf, 2.0, 0.1),
+                     damping=P.CombinedDamping(0.1, kf, 1e-8 * (1024 / N) ** 8, 8), noise=phases)
+    err = rel(st["theta_hat"].to(torch.complex128), sto["theta_hat"])
+    assert err < 2e-5, err
+
+
 def test_deterministic_replay(P):
     g = P.make_grid(256, TWO_PI)
     s = P.gSQGSolver(g, 1.0, 0.0, 8, precision="float32", scheme="ifrk4")
