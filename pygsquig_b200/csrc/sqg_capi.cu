@@ -248,9 +248,13 @@ KP make_kp(const sqg_plan* pl, double dt) {
 // ---- compile-time launch shapes ----
 // Radix of the group FFTs.  Column pass: 16 for float grids with N >= 2048
 // (groups of N/16 threads, one exchange pass fewer, two 256-thread blocks per
-// SM; measured at N = 4096: 370 -> 271 us per launch); row pass: 8 (radix 16
-// with two exchange buffers made the fused stage pass slower, 384 -> 508 us,
-// because its stage update walks 16 prefetched chunks per thread).
+// SM; measured at N = 4096: 370 -> 271 us per launch); row pass: 8 at those
+// sizes (radix 16 with two exchange buffers made the fused stage pass slower,
+// 384 -> 508 us, because its stage update walks 16 prefetched chunks per
+// thread).  Float grids with 128 <= N <= 1024: radix-4 row pass (the pass is
+// one wave of blocks bound by each block's latency; twice the threads per
+// transform at 64 registers: N = 1024 row passes 31 -> 20 us); the column
+// pass stays radix 8 there (radix 4 took 23 -> 30 us at N = 1024).
 template <typename T, int L>
 constexpr int col_radix() { return (sizeof(T) == 4 && L >= 11) ? 16 : 8; }
 template <typename T, int L>
@@ -301,7 +305,7 @@ constexpr size_t row_pf_bytes(int depth) {
 // per block), the deepest among equals: occupancy first, then prefetch depth.
 template <typename T, int L>
 constexpr int row_occupancy(int depth) {
-  constexpr int by_regs = row_min_blocks<T, row_radix<T, L>()>(rows_per_cta<T, L>() * row_group<T, L>());
+  constexpr int by_regs = min_blocks_r<T, row_radix<T, L>()>(rows_per_cta<T, L>() * row_group<T, L>());
   const size_t smem = row_base_smem<T, L>() + row_pf_bytes<T, L>(depth);
   if (smem > 220 * 1024) return 0;
   const int by_smem = (int)((227 * 1024) / (smem + 1024));

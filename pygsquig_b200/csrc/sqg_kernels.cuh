@@ -109,10 +109,10 @@ constexpr int min_blocks(int threads) {
   return sizeof(T) == 4 ? (65536 / (threads * 128) > 8 ? 8 : (65536 / (threads * 128) > 0 ? 65536 / (threads * 128) : 1))
                         : (65536 / (threads * 168) > 8 ? 8 : (65536 / (threads * 168) > 0 ? 65536 / (threads * 168) : 1));
 }
-// Row pass: radix 4 (single precision, N <= 1024) keeps few values per thread,
-// so its blocks are held to 64 registers a thread (twice the resident warps).
+// Radix-4 passes (single precision, N <= 1024) keep few values per thread, so
+// their blocks are held to 64 registers a thread (twice the resident warps).
 template <typename T, int R>
-constexpr int row_min_blocks(int threads) {
+constexpr int min_blocks_r(int threads) {
   return (R == 4 && sizeof(T) == 4) ? (65536 / (threads * 64) > 8 ? 8 : (65536 / (threads * 64) > 0 ? 65536 / (threads * 64) : 1))
                                     : min_blocks<T>(threads);
 }
@@ -878,14 +878,14 @@ __global__ void k_set_ctl(RingCtl* ctl, const double* base) {
 namespace sqg {
 // ---- kernels: one plan, or a batch of members (member = blockIdx.y) ----
 template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
-__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), row_min_blocks<T, R>(RPC * ((1 << LOG2N) / R)))
+__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), min_blocks_r<T, R>(RPC * ((1 << LOG2N) / R)))
 k_row(KP kp, RowArgs a) {
   pdl_wait();
   row_body<T, LOG2N, R, RPC, DEPTH, NFX>(kp, a);
 }
 
 template <typename T, int LOG2N, int R, int NP, int NBUF>
-__global__ void __launch_bounds__(NP * ((1 << LOG2N) / R), min_blocks<T>(NP * ((1 << LOG2N) / R)))
+__global__ void __launch_bounds__(NP * ((1 << LOG2N) / R), min_blocks_r<T, R>(NP * ((1 << LOG2N) / R)))
 k_col(KP kp, ColArgs a) {
   pdl_wait();
   col_body<T, LOG2N, R, NP, NBUF>(kp, a);
@@ -894,7 +894,7 @@ k_col(KP kp, ColArgs a) {
 // Batched forms: the member's parameters come from device arrays; members
 // with no work in this pass have a null xh pointer and return at once.
 template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
-__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), row_min_blocks<T, R>(RPC * ((1 << LOG2N) / R)))
+__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), min_blocks_r<T, R>(RPC * ((1 << LOG2N) / R)))
 k_row_batch(const KP* __restrict__ kps, const RowArgs* __restrict__ as) {
   pdl_wait();
   const KP kp = kps[blockIdx.y];
@@ -904,7 +904,7 @@ k_row_batch(const KP* __restrict__ kps, const RowArgs* __restrict__ as) {
 }
 
 template <typename T, int LOG2N, int R, int NP, int NBUF>
-__global__ void __launch_bounds__(NP * ((1 << LOG2N) / R), min_blocks<T>(NP * ((1 << LOG2N) / R)))
+__global__ void __launch_bounds__(NP * ((1 << LOG2N) / R), min_blocks_r<T, R>(NP * ((1 << LOG2N) / R)))
 k_col_batch(const KP* __restrict__ kps, const ColArgs* __restrict__ as) {
   pdl_wait();
   const KP kp = kps[blockIdx.y];
