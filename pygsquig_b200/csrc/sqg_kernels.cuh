@@ -109,8 +109,8 @@ constexpr int min_blocks(int threads) {
   return sizeof(T) == 4 ? (65536 / (threads * 128) > 8 ? 8 : (65536 / (threads * 128) > 0 ? 65536 / (threads * 128) : 1))
                         : (65536 / (threads * 168) > 8 ? 8 : (65536 / (threads * 168) > 0 ? 65536 / (threads * 168) : 1));
 }
-// Radix-4 passes (single precision, N <= 1024) keep few values per thread, so
-// their blocks are held to 64 registers a thread (twice the resident warps).
+// Radix-4 passes (single precision) keep few values per thread, so their
+// blocks are held to 64 registers a thread (twice the resident warps).
 template <typename T, int R>
 constexpr int min_blocks_r(int threads) {
   return (R == 4 && sizeof(T) == 4) ? (65536 / (threads * 64) > 8 ? 8 : (65536 / (threads * 64) > 0 ? 65536 / (threads * 64) : 1))
