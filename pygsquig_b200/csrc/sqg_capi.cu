@@ -259,7 +259,7 @@ KP make_kp(const sqg_plan* pl, double dt) {
 template <typename T, int L>
 constexpr int col_radix() { return (sizeof(T) == 4 && L >= 11) ? 16 : 8; }
 template <typename T, int L>
-constexpr int row_radix() { return (sizeof(T) == 4 && L >= 7 && L <= 11) ? 4 : 8; }
+constexpr int row_radix() { return (L >= 7 && L <= (sizeof(T) == 4 ? 11 : 10)) ? 4 : 8; }
 template <typename T, int L>
 constexpr int row_group() { return (1 << L) / row_radix<T, L>(); }
 template <typename T, int L>

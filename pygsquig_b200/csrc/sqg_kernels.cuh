@@ -109,12 +109,14 @@ constexpr int min_blocks(int threads) {
   return sizeof(T) == 4 ? (65536 / (threads * 128) > 8 ? 8 : (65536 / (threads * 128) > 0 ? 65536 / (threads * 128) : 1))
                         : (65536 / (threads * 168) > 8 ? 8 : (65536 / (threads * 168) > 0 ? 65536 / (threads * 168) : 1));
 }
-// Radix-4 passes (single precision) keep few values per thread, so their
-// blocks are held to 64 registers a thread (twice the resident warps).
+// Radix-4 passes keep few values per thread, so their blocks are held to 64
+// registers a thread in single precision and 128 in double (more resident
+// warps than the radix-8 pass at the same size).
 template <typename T, int R>
 constexpr int min_blocks_r(int threads) {
-  return (R == 4 && sizeof(T) == 4) ? (65536 / (threads * 64) > 8 ? 8 : (65536 / (threads * 64) > 0 ? 65536 / (threads * 64) : 1))
-                                    : min_blocks<T>(threads);
+  constexpr int regs = sizeof(T) == 4 ? 64 : 128;
+  return R == 4 ? (65536 / (threads * regs) > 8 ? 8 : (65536 / (threads * regs) > 0 ? 65536 / (threads * regs) : 1))
+                : min_blocks<T>(threads);
 }
 
 __device__ __forceinline__ int mode_abs(int i, int N) { return i <= (N >> 1) ? i : N - i; }
