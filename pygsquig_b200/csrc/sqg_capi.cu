@@ -251,15 +251,17 @@ KP make_kp(const sqg_plan* pl, double dt) {
 // SM; measured at N = 4096: 370 -> 271 us per launch); row pass: 8 at those
 // sizes (radix 16 with two exchange buffers made the fused stage pass slower,
 // 384 -> 508 us, because its stage update walks 16 prefetched chunks per
-// thread).  Float grids with 128 <= N <= 2048: radix-4 row pass (twice the
-// threads per transform at 64 registers; at N <= 1024 the pass is one wave
-// of blocks bound by each block's latency: N = 1024 row passes 31 -> 20 us,
-// N = 2048 step 0.64 -> 0.57 ms; at N = 4096 it was slower, 315 -> 357 us);
-// the column pass stays radix 8 there (radix 4 took 23 -> 30 us at N = 1024).
+// thread).  Grids with 128 <= N <= 2048: radix-4 row pass (twice the threads
+// per transform at 64 registers in single precision, 128 in double; at
+// N <= 1024 the pass is one wave of blocks bound by each block's latency:
+// FP32 N = 1024 row passes 31 -> 20 us, FP64 52 -> 36 us; N = 2048 step
+// FP32 0.64 -> 0.57 ms, FP64 1.36 -> 1.19 ms; at N = 4096 it was slower,
+// 315 -> 357 us); the column pass stays radix 8 there (radix 4 took
+// 23 -> 30 us at N = 1024).
 template <typename T, int L>
 constexpr int col_radix() { return (sizeof(T) == 4 && L >= 11) ? 16 : 8; }
 template <typename T, int L>
-constexpr int row_radix() { return (L >= 7 && L <= (sizeof(T) == 4 ? 11 : 10)) ? 4 : 8; }
+constexpr int row_radix() { return (L >= 7 && L <= 11) ? 4 : 8; }
 template <typename T, int L>
 constexpr int row_group() { return (1 << L) / row_radix<T, L>(); }
 template <typename T, int L>
