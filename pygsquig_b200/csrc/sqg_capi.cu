@@ -257,7 +257,7 @@ KP make_kp(const sqg_plan* pl, double dt) {
 // FP32 N = 1024 row passes 31 -> 20 us, FP64 52 -> 36 us; N = 2048 step
 // FP32 0.64 -> 0.57 ms, FP64 1.36 -> 1.19 ms; at N = 4096 it was slower,
 // 315 -> 357 us); the column pass stays radix 8 there (radix 4 took
-// 23 -> 30 us at N = 1024).
+// 23 -> 30 us at N = 1024 in single precision, 34 -> 39 us in double).
 template <typename T, int L>
 constexpr int col_radix() { return (sizeof(T) == 4 && L >= 11) ? 16 : 8; }
 template <typename T, int L>
