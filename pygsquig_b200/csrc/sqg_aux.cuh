@@ -259,8 +259,8 @@ __global__ void __launch_bounds__(256) k_ring_substeps(int N, int n, const int* 
                                                        typename Cplx<T>::type* theta, double2* F) {
   pdl_wait();
   using C = typename Cplx<T>::type;
-  constexpr int V = 256;
-  __shared__ double red_r[V], red_q[V];
+  constexpr int V = 256;  // launched with exactly V threads
+  __shared__ double red_r[V / 32], red_q[V / 32];
   __shared__ double s_c;
   const int ho[4] = {herm_ord.x, herm_ord.y, herm_ord.z, herm_ord.w};
   const double inv_n4 = 1.0 / ((double)N * N * (double)N * N);
@@ -275,33 +275,38 @@ __global__ void __launch_bounds__(256) k_ring_substeps(int N, int n, const int* 
       F[i] = make_double2(amp * cs, fy);
     }
     __syncthreads();
-    for (int v = threadIdx.x; v < V; v += blockDim.x) {
-      double ar = 0.0, aq = 0.0;
-      for (int i = v; i < n; i += V) {
-        const int pos = ring_pos[i];
-        const int ix = pos / N, iy = pos - ix * N;
-        const int mpos = ((N - ix) & (N - 1)) * N + ((N - iy) & (N - 1));
-        const C t1 = theta[pos], t2 = theta[mpos];
-        const double hx = 0.5 * ((double)t1.x + (double)t2.x);
-        const double hy = 0.5 * ((double)t1.y - (double)t2.y);
-        const double2 f1 = F[i], f2 = F[ring_mirror[i]];
-        const double fx = 0.5 * (f1.x + f2.x), fy = 0.5 * (f1.y - f2.y);
-        ar += hx * fx + hy * fy;
-        aq += fx * fx + fy * fy;
-      }
-      red_r[v] = ar;
-      red_q[v] = aq;
+    // fixed-order reduction: each thread sums its strided modes, warps
+    // reduce by shuffles, thread 0 adds the eight warp sums in order
+    double ar = 0.0, aq = 0.0;
+    for (int i = threadIdx.x; i < n; i += V) {
+      const int pos = ring_pos[i];
+      const int ix = pos / N, iy = pos - ix * N;
+      const int mpos = ((N - ix) & (N - 1)) * N + ((N - iy) & (N - 1));
+      const C t1 = theta[pos], t2 = theta[mpos];
+      const double hx = 0.5 * ((double)t1.x + (double)t2.x);
+      const double hy = 0.5 * ((double)t1.y - (double)t2.y);
+      const double2 f1 = F[i], f2 = F[ring_mirror[i]];
+      const double fx = 0.5 * (f1.x + f2.x), fy = 0.5 * (f1.y - f2.y);
+      ar += hx * fx + hy * fy;
+      aq += fx * fx + fy * fy;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ar += __shfl_down_sync(0xffffffffu, ar, o);
+      aq += __shfl_down_sync(0xffffffffu, aq, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      red_r[threadIdx.x >> 5] = ar;
+      red_q[threadIdx.x >> 5] = aq;
     }
     __syncthreads();
-    for (int w = V / 2; w > 0; w >>= 1) {
-      for (int v = threadIdx.x; v < w; v += blockDim.x) {
-        red_r[v] += red_r[v + w];
-        red_q[v] += red_q[v + w];
-      }
-      __syncthreads();
-    }
     if (threadIdx.x == 0) {
-      const double r1 = red_r[0] * inv_n4, q = red_q[0] * inv_n4;
+      double sr = 0.0, sq = 0.0;
+      for (int w = 0; w < V / 32; ++w) {
+        sr += red_r[w];
+        sq += red_q[w];
+      }
+      const double r1 = sr * inv_n4, q = sq * inv_n4;
       auto sc = [&](double r) { return fabs(r) > 1e-10 ? eps / r : 1.0; };
       const double s1 = sc(r1);
       const double s2 = sc(r1 + 0.5 * dt * s1 * q);
