@@ -326,6 +326,32 @@ constexpr int row_depth() {
 }
 template <typename T, int L>
 size_t row_smem() { return row_base_smem<T, L>() + row_pf_bytes<T, L>(row_depth<T, L>()); }
+// The stage pass without inverse transforms (the last stage of a step): one
+// exchange buffer per row pair, registers as row_min_blocks<.., 1>; prefetch
+// depth again occupancy first.
+template <typename T, int L>
+constexpr size_t rowx_smem(int depth) {
+  return (size_t)rows_per_cta<T, L>() * spad_size<row_radix<T, L>()>(1 << L) * sizeof(typename Cplx<T>::type) +
+         row_pf_bytes<T, L>(depth);
+}
+template <typename T, int L>
+constexpr int rowx_occupancy(int depth) {
+  constexpr int by_regs = row_min_blocks<T, row_radix<T, L>(), 1>(rows_per_cta<T, L>() * row_group<T, L>());
+  const size_t smem = rowx_smem<T, L>(depth);
+  if (smem > 220 * 1024) return 0;
+  const int by_smem = (int)((227 * 1024) / (smem + 1024));
+  return by_smem < by_regs ? by_smem : by_regs;
+}
+template <typename T, int L>
+constexpr int rowx_depth() {
+  constexpr int R = row_radix<T, L>();
+  int best = 1, occ = rowx_occupancy<T, L>(1);
+  for (int d = 2; d <= R; d *= 2) {
+    const int o = rowx_occupancy<T, L>(d);
+    if (o >= occ && o > 0) { occ = o; best = d; }
+  }
+  return best;
+}
 template <typename T, int L>
 size_t col_smem() {  // per column pair: NBUF buffers plus the slack of col_qstride
   return (size_t)pairs_per_cta<T, L>() *
@@ -345,6 +371,9 @@ cudaError_t launch_row_t(const KP& kp, const RowArgs& a, cudaStream_t st) {
   constexpr int N = 1 << L, RPC = rows_per_cta<T, L>();
   const int rpc = a.rpc > 0 ? a.rpc : RPC;
   const int grid = (N / 2 + 1 + rpc - 1) / rpc;
+  if (a.rmode == RM_STAGE && !a.do_p1)
+    return launch_pdl(k_row<T, L, row_radix<T, L>(), RPC, rowx_depth<T, L>(), 1>, dim3(grid),
+                      dim3(rpc * row_group<T, L>()), rowx_smem<T, L>(rowx_depth<T, L>()) / RPC * rpc, st, kp, a);
   return launch_pdl(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>, dim3(grid),
                     dim3(rpc * row_group<T, L>()), row_smem<T, L>() / RPC * rpc, st, kp, a);
 }
@@ -367,6 +396,9 @@ cudaError_t set_attrs_t() {
   constexpr int RPC = rows_per_cta<T, L>(), NP = pairs_per_cta<T, L>();
   cudaError_t e = cudaFuncSetAttribute(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem<T, L>());
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_row<T, L, row_radix<T, L>(), RPC, rowx_depth<T, L>(), 1>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rowx_smem<T, L>(rowx_depth<T, L>()));
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem<T, L>());

@@ -119,6 +119,14 @@ constexpr int min_blocks_r(int threads) {
                 : min_blocks<T>(threads);
 }
 
+// Row-pass blocks: the pass without the inverse transforms (NFX = 1) is held
+// to the radix-4 register budget (64 a thread in single precision, 128 in
+// double), so that more of its blocks fit than of the full pass.
+template <typename T, int R, int NFX>
+constexpr int row_min_blocks(int threads) {
+  return NFX == 1 ? min_blocks_r<T, 4>(threads) : min_blocks_r<T, R>(threads);
+}
+
 __device__ __forceinline__ int mode_abs(int i, int N) { return i <= (N >> 1) ? i : N - i; }
 
 // |k|^-alpha with k = 0 -> 0 (operators.py:134-155)
@@ -477,6 +485,12 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a) {
   if (kp.status) {
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(kp.status, 1u);
   }
+  // NFX = 1 is the instantiation for stage passes without the inverse
+  // transforms (the last stage of a step): compiled without them, it needs
+  // few registers and one exchange buffer, so two blocks share an SM.
+  if constexpr (NFX < 2) {
+    return;
+  } else {
   if (!a.do_p1) return;
 
   // Rows 0 and N/2 pair with themselves: e2 = (p, N - iy) is owned by another
@@ -505,6 +519,7 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a) {
     row_fields<T, LOG2N, R, 1>(kp, a, t1, t2, 0, j, p, valid, wbuf);
   } else {
     row_fields<T, LOG2N, R, 2>(kp, a, t1, t2, 0, j, p, valid, wbuf);
+  }
   }
 }
 
@@ -880,7 +895,7 @@ __global__ void k_set_ctl(RingCtl* ctl, const double* base) {
 namespace sqg {
 // ---- kernels: one plan, or a batch of members (member = blockIdx.y) ----
 template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
-__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), min_blocks_r<T, R>(RPC * ((1 << LOG2N) / R)))
+__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), row_min_blocks<T, R, NFX>(RPC * ((1 << LOG2N) / R)))
 k_row(KP kp, RowArgs a) {
   pdl_wait();
   row_body<T, LOG2N, R, RPC, DEPTH, NFX>(kp, a);
@@ -896,7 +911,7 @@ k_col(KP kp, ColArgs a) {
 // Batched forms: the member's parameters come from device arrays; members
 // with no work in this pass have a null xh pointer and return at once.
 template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
-__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), min_blocks_r<T, R>(RPC * ((1 << LOG2N) / R)))
+__global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), row_min_blocks<T, R, NFX>(RPC * ((1 << LOG2N) / R)))
 k_row_batch(const KP* __restrict__ kps, const RowArgs* __restrict__ as) {
   pdl_wait();
   const KP kp = kps[blockIdx.y];
