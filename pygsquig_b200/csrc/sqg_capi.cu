@@ -272,6 +272,9 @@ template <typename T, int L>
 constexpr int pairs_per_cta() {
   constexpr int g = col_group<T, L>();
   constexpr int cap = (1 << L) / 2 < 16 ? (1 << L) / 2 : 16;
+  // radix 16: up to two column pairs (four columns fill the 32-byte sectors
+  // of each row's gather); the autotuner picks one or two
+  if (col_radix<T, L>() == 16) return 2;
   return g >= 256 ? 1 : (256 / g > cap ? cap : 256 / g);
 }
 // Four resident field buffers per column pair when they fit in 150 KB; the
