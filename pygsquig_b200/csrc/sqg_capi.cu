@@ -279,8 +279,8 @@ constexpr int pairs_per_cta() {
 }
 // Four resident field buffers per column pair when they fit in 150 KB; the
 // radix-16 column pass (FP32, N >= 2048) keeps two (two rounds of two fields,
-// 256-thread blocks of about 67 KB, so that two or three blocks share an SM
-// and one block's loads overlap another's transforms).
+// about 35 KB a buffer: one or two column pairs per block as the autotuner
+// chose, 70 or 140 KB).
 template <typename T, int L>
 constexpr int col_nbuf() {
   return col_radix<T, L>() == 16 ? 2
@@ -289,7 +289,7 @@ constexpr int col_nbuf() {
 }
 // Exchange buffers of the row pass: four (the theta fields transform
 // together) when they fit in 150 KB, else two (two rounds); two for a
-// radix-16 row pass.
+// radix-4 or radix-16 row pass.
 template <typename T, int L>
 constexpr int row_nfx() {
   return row_radix<T, L>() != 8 ? 2
