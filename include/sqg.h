@@ -133,12 +133,15 @@ int sqg_rhs(sqg_plan* plan, const void* theta_hat, void* rhs, void* stream);
  * workspace: the grid tables and intermediate fields live in a static device
  * array of SQG_NOALLOC_SCRATCH_BYTES (3 MiB) that every GPU loading the
  * library keeps until the process exits.  Limit: N <= SQG_NOALLOC_MAX_N (256),
- * larger N is rejected with SQG_ERR_INVALID.  The first call on a device
- * resolves the array's device address (cudaGetSymbolAddress) for that
- * device; make that first call before any stream capture.  Every call
- * rewrites the whole array, so calls that overlap on the GPU (other streams,
- * other host threads) race and must be serialised by the caller.  Only N, L,
- * alpha, nu_p, p and precision of the descriptor are used. */
+ * larger N is rejected with SQG_ERR_INVALID.  Each call looks up the array's
+ * device address on the current device (cudaGetSymbolAddress); the first
+ * call on a device also loads the library's device code there, so make that
+ * first call before any stream capture.  Every call rewrites the whole
+ * array, so calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller.  Only N, L, alpha,
+ * nu_p, p and precision of the descriptor are used.  The twiddle table is
+ * computed on the device here (on the host for a plan), so the result equals
+ * sqg_rhs's to rounding, not bit for bit. */
 #define SQG_NOALLOC_MAX_N 256
 #define SQG_NOALLOC_SCRATCH_BYTES (3u << 20)
 int sqg_rhs_noalloc(const sqg_desc* desc, const void* theta_hat, void* rhs, void* stream);

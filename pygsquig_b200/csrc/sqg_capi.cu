@@ -604,11 +604,12 @@ const char* sqg_last_error_string(void) { return g_last_error.c_str(); }
 int sqg_plan_create(const sqg_desc* desc, sqg_plan** out) {
   if (!desc || !out) return fail(SQG_ERR_INVALID, "null argument");
   const sqg_desc& d = *desc;
+  if (d.N % 2 != 0) return fail(SQG_ERR_INVALID, "N must be even, got " + std::to_string(d.N));
+  // range first: the power-of-two search below then never shifts past bit 12
+  if (d.N < 8 || d.N > 4096 || (d.N & (d.N - 1)) != 0)
+    return fail(SQG_ERR_INVALID, "N must be a power of two in [8, 4096], got " + std::to_string(d.N));
   int log2n = 0;
   while ((1 << log2n) < d.N) ++log2n;
-  if (d.N % 2 != 0) return fail(SQG_ERR_INVALID, "N must be even, got " + std::to_string(d.N));
-  if ((1 << log2n) != d.N || d.N < 8 || d.N > 4096)
-    return fail(SQG_ERR_INVALID, "N must be a power of two in [8, 4096], got " + std::to_string(d.N));
   if (!(d.alpha >= -2 && d.alpha <= 2)) return fail(SQG_ERR_INVALID, "alpha must be in [-2, 2], got " + std::to_string(d.alpha));
   if (d.p != 2 && d.p != 4 && d.p != 8) return fail(SQG_ERR_INVALID, "p must be 2, 4, or 8, got " + std::to_string(d.p));
   if (d.has_damping && d.p_damp != 2 && d.p_damp != 4 && d.p_damp != 8)
@@ -1327,9 +1328,6 @@ namespace {
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[SQG_NOALLOC_SCRATCH_BYTES];
 
-constexpr int kMaxDevices = 64;
-void* g_noalloc_dev_ptr[kMaxDevices] = {};  // device address of g_noalloc_scratch, per device
-
 // Grid tables of the no-allocation path, computed on the device with the
 // same float64 expressions the host path uses (round-to-nearest intrinsics
 // keep the compiler from contracting them into FMAs, so the dealiasing mask
@@ -1384,9 +1382,7 @@ cudaError_t noalloc_tables(int N, double L, unsigned char* base, size_t o_k1d, s
 extern "C" int sqg_rhs_noalloc(const sqg_desc* desc, const void* theta, void* rhs, void* stream) {
   if (!desc || !theta || !rhs) return fail(SQG_ERR_INVALID, "null argument");
   const sqg_desc& d = *desc;
-  int log2n = 0;
-  while ((1 << log2n) < d.N) ++log2n;
-  if ((1 << log2n) != d.N || d.N < 8 || d.N > SQG_NOALLOC_MAX_N)
+  if (d.N < 8 || d.N > SQG_NOALLOC_MAX_N || (d.N & (d.N - 1)) != 0)
     return fail(SQG_ERR_INVALID, "sqg_rhs_noalloc: N must be a power of two in [8, " +
                                      std::to_string(SQG_NOALLOC_MAX_N) + "] (static scratch of " +
                                      std::to_string(SQG_NOALLOC_SCRATCH_BYTES >> 20) + " MiB), got " +
@@ -1395,18 +1391,19 @@ extern "C" int sqg_rhs_noalloc(const sqg_desc* desc, const void* theta, void* rh
   if (d.p != 2 && d.p != 4 && d.p != 8) return fail(SQG_ERR_INVALID, "p must be 2, 4, or 8, got " + std::to_string(d.p));
   if (d.precision != SQG_F64 && d.precision != SQG_F32) return fail(SQG_ERR_INVALID, "bad precision");
   if (!(d.L > 0)) return fail(SQG_ERR_INVALID, "L must be positive");
-  int dev = 0;
-  SQG_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) return fail(SQG_ERR_INVALID, "device index out of range");
-  // One-time set-up per device (the current one): the device address of the
-  // static array.  In host code the array's name is only a host-side stand-in.
-  if (!g_noalloc_dev_ptr[dev]) {
-    void* p = nullptr;
-    SQG_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    g_noalloc_dev_ptr[dev] = p;
-  }
-  // A plan that lives on the stack and points into the static scratch.
-  sqg_plan pl;
+  int log2n = 0;
+  while ((1 << log2n) < d.N) ++log2n;
+  // The device address of the static array on the current device.  In host
+  // code the array's name is only a host-side stand-in, never a device
+  // address.  It is looked up on every call (a host-side table lookup once
+  // the module is loaded), so no per-device cache can race between host
+  // threads or go stale after a cudaDeviceReset; the first call on a device
+  // loads the module and belongs before any stream capture.
+  void* scratch = nullptr;
+  SQG_CUDA(cudaGetSymbolAddress(&scratch, g_noalloc_scratch));
+  // A plan that lives on the stack and points into the static scratch
+  // (value-initialised: every offset and flag not set below is zero).
+  sqg_plan pl{};
   pl.d = d;
   pl.d.has_damping = 0;
   pl.d.has_ring = 0;
@@ -1429,7 +1426,7 @@ extern "C" int sqg_rhs_noalloc(const sqg_desc* desc, const void* theta, void* rh
   pl.off_jh = take(half);
   pl.off_acc = pl.off_stage = pl.off_xh;  // unused by the RHS passes
   if (o > SQG_NOALLOC_SCRATCH_BYTES) return fail(SQG_ERR_INVALID, "sqg_rhs_noalloc: scratch too small");
-  pl.ws = (unsigned char*)g_noalloc_dev_ptr[dev];
+  pl.ws = (unsigned char*)scratch;
   pl.ws_bytes = SQG_NOALLOC_SCRATCH_BYTES;
   pl.ready = true;
   cudaStream_t st = (cudaStream_t)stream;

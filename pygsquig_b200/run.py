@@ -27,6 +27,7 @@ Differences that come from running on the GPU:
 
 from __future__ import annotations
 
+import logging
 import math
 import signal
 import time
@@ -44,7 +45,7 @@ from .forcing import CombinedDamping, RingForcing
 from .io import load_checkpoint, load_config, save_checkpoint, save_diagnostics, save_output
 from .io.checkpoint import h5py
 from .utils.diagnostics import compute_enstrophy, compute_total_energy
-from .utils.logging import setup_logging
+from .utils.runlog import RunLog
 
 _shutdown = {"requested": False}
 
@@ -66,7 +67,7 @@ def setup_output_directories(output_dir: Path, config, logger) -> dict:
     for d in dirs.values():
         d.mkdir(exist_ok=True)
     config.to_yaml(output_dir / "config.yml")
-    logger.info(f"Configuration saved to {output_dir / 'config.yml'}")
+    logger.event("config", file=str(output_dir / "config.yml"))
     return dirs
 
 
@@ -107,31 +108,28 @@ def initialize_simulation(config, checkpoint_path, logger, precision="float64", 
                    for s in config.scalars.species}
         solver = gSQGSolverWithScalars(grid, sc.alpha, sc.dissipation.nu_p, sc.dissipation.p,
                                        passive_scalars=species, **kw)
-        logger.info(f"Initialized solver with {len(species)} passive scalar(s)")
+        logger.event("solver", alpha=sc.alpha, scalars=len(species), precision=precision, scheme=scheme)
     else:
         solver = gSQGSolver(grid, sc.alpha, sc.dissipation.nu_p, sc.dissipation.p, **kw)
     ic = config.initial_condition
     if checkpoint_path is None and ic.type == "checkpoint":
         checkpoint_path = ic.checkpoint_path
     if checkpoint_path:
-        logger.info(f"Loading checkpoint: {checkpoint_path}")
         state, _ = load_checkpoint(checkpoint_path)
         state["theta_hat"] = state["theta_hat"].to(solver.cdtype).cuda()
-        logger.info(f"Resuming from t={state['time']:.2f}, step={state['step']}")
+        logger.event("resume", file=str(checkpoint_path), t=float(state["time"]), step=int(state["step"]))
         return grid, solver, state
     scal = None
     if config.scalars and config.scalars.enabled:
         scal = {s.name: _scalar_field(s, grid, ic.seed) for s in config.scalars.species}
     if ic.type == "random":
         kw0 = dict(seed=ic.seed)
-        msg = f"Initialized with random initial condition (seed={ic.seed})"
     elif ic.type == "zero":
         kw0 = dict(theta0=np.zeros((grid.N, grid.N)))
-        msg = "Initialized with zero initial condition"
     else:
         raise NotImplementedError(f"Initial condition type '{ic.type}' not implemented")
     state = solver.initialize(scalar_init=scal, **kw0) if scal is not None else solver.initialize(**kw0)
-    logger.info(msg + (f" and {len(scal)} scalar(s)" if scal else ""))
+    logger.event("initial", kind=ic.type, seed=ic.seed, scalars=len(scal) if scal else 0)
     return grid, solver, state
 
 
@@ -161,7 +159,7 @@ def _fields(state, grid, config, logger, solver):
         if f == "theta":
             data["theta"] = ifft2(th_hat)
         elif f == "vorticity":
-            logger.warning("Vorticity output not yet implemented")
+            logger.event("skip_field", logging.WARNING, field="vorticity", why="not produced by this driver")
         elif f == "streamfunction":
             data["streamfunction"] = ifft2(compute_streamfunction(th_hat, grid, config.solver.alpha))
         elif f == "velocity":
@@ -184,7 +182,7 @@ class Driver:
             self.ring = RingForcing(kf=fc.kf, dk=fc.dk, epsilon=fc.epsilon, tau_f=fc.tau_f)
             self.rng = np.random.default_rng(fc.seed if fc.seed else 42)
             self.n_ring = self.ring.n_modes(grid)
-            logger.info(f"Initialized ring forcing: kf={fc.kf}, ε={fc.epsilon}")
+            logger.event("forcing", kind="ring", kf=fc.kf, dk=fc.dk, eps=fc.epsilon, tau_f=fc.tau_f)
         self.damping = None
         dc = config.solver.damping
         if dc and dc.type != "none":
@@ -192,7 +190,7 @@ class Driver:
             # a second hyperviscous term on top of the solver's own
             self.damping = CombinedDamping(mu=dc.mu, kf=fc.kf if fc else 20.0,
                                            nu_p=config.solver.dissipation.nu_p, p=config.solver.dissipation.p)
-            logger.info(f"Initialized damping: μ={dc.mu}")
+            logger.event("damping", mu=dc.mu, kf=fc.kf if fc else 20.0, nu_p=config.solver.dissipation.nu_p)
 
     # -- one adaptive or clamped step --
     def _dt(self) -> float:
@@ -250,7 +248,7 @@ class Driver:
                 el = time.time() - t_start_wall
                 rate = (now - last_log) / (time.time() - t_start_wall + el) if now > last_log else 0
                 eta = (t_end - now) / rate if rate > 0 else None
-                self.log.log_progress(now, self.state["step"], dt, d, eta)
+                self.log.progress(now, self.state["step"], dt, d, eta)
                 save_diagnostics(d, now, self.dirs["diagnostics"] / ("timeseries" + _ext("diag")))
                 last_log = now
             if now - last_out >= sim.output_interval:
@@ -260,16 +258,16 @@ class Driver:
                         "nu_p": float(cfg.solver.dissipation.nu_p), "p": int(cfg.solver.dissipation.p)}
                 save_output(_fields(self.state, self.grid, cfg, self.log, self.solver), self.grid, now, meta, f,
                             compress=cfg.output.compress)
-                self.log.log_output(f, now, step)
+                self.log.wrote("fields", f, now, step)
                 last_out = now
             if now - last_ckpt >= sim.checkpoint_interval:
                 step = self.state["step"]
                 f = self.dirs["checkpoints"] / f"step_{step:08d}{_ext('ckpt')}"
                 save_checkpoint(self.state, cfg, f)
-                self.log.log_checkpoint(f, now, step)
+                self.log.wrote("checkpoint", f, now, step)
                 last_ckpt = now
             if sim.wall_time_limit and time.time() - t_start_wall > sim.wall_time_limit:
-                self.log.warning("Wall time limit reached!")
+                self.log.event("wall_limit", logging.WARNING, limit_s=sim.wall_time_limit)
                 _shutdown["requested"] = True
         return last_out
 
@@ -280,14 +278,10 @@ def run(config_path, checkpoint=None, output_dir="./output", dry_run=False, log_
     out = Path(output_dir)
     if not dry_run:
         out.mkdir(parents=True, exist_ok=True)
-    logger = setup_logging(out if not dry_run else None, console_level=log_level)
-    logger.info(f"Loading configuration: {config_path}")
+    logger = RunLog(out if not dry_run else None, level=log_level)
+    logger.event("config", file=str(config_path), N=cfg.grid.N, L=cfg.grid.L, alpha=cfg.solver.alpha,
+                 t_end=cfg.simulation.t_end, dry_run=bool(dry_run))
     if dry_run:
-        logger.info("Dry run mode - validating configuration only")
-        logger.info("Configuration validated successfully!")
-        logger.info(f"Grid: {cfg.grid.N}x{cfg.grid.N}, L={cfg.grid.L}")
-        logger.info(f"Solver: α={cfg.solver.alpha}")
-        logger.info(f"Simulation time: {cfg.simulation.t_end}")
         return None
     if not torch.cuda.is_available():
         raise RuntimeError("pygsquig_b200.run needs a CUDA device (the solver has no CPU path)")
@@ -295,19 +289,16 @@ def run(config_path, checkpoint=None, output_dir="./output", dry_run=False, log_
     _shutdown["requested"] = False
     old = signal.signal(signal.SIGINT, _on_sigint)
     try:
-        logger.info("Initializing simulation...")
         grid, solver, state = initialize_simulation(cfg, checkpoint, logger, precision, scheme)
-        logger.log_simulation_start(cfg, f"cuda ({torch.cuda.get_device_name()})")
-        logger.info(f"Starting simulation from t={state['time']:.2f} to t={cfg.simulation.t_end:.2f}")
+        logger.started(cfg, f"cuda ({torch.cuda.get_device_name()})")
         t_wall = time.time()
         drv = Driver(cfg, grid, solver, state, dirs, logger)
         last_out = drv.run(t_wall)
         state = drv.state
-        logger.info("Saving final state...")
         step, now = state["step"], state["time"]
         f = dirs["checkpoints"] / f"final_step_{step:08d}{_ext('ckpt')}"
         save_checkpoint(state, cfg, f)
-        logger.info(f"Final checkpoint saved: {f}")
+        logger.wrote("checkpoint", f, now, step)
         if now - last_out > 0:
             data = {"theta": ifft2(state["theta_hat"])}
             if state.get("scalar_state") is not None:
@@ -315,9 +306,8 @@ def run(config_path, checkpoint=None, output_dir="./output", dry_run=False, log_
                     data[f"scalar_{name}"] = ifft2(sh)
             f = dirs["fields"] / f"fields_final_{step:08d}{_ext('fields')}"
             save_output(data, grid, now, {"step": int(step)}, f)
-            logger.info(f"Final output saved: {f}")
-        logger.log_simulation_complete(now, step, time.time() - t_wall)
-        logger.info(f"Output saved to: {out}")
+            logger.wrote("fields", f, now, step)
+        logger.finished(now, step, time.time() - t_wall)
         return state
     finally:
         signal.signal(signal.SIGINT, old)
