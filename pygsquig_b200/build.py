@@ -20,13 +20,16 @@ import time
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
-SRCS = [os.path.join(CSRC, f) for f in ("sqg_capi.cu", "closure_conv.cu", "closure_ops.cu")]
+_INST = [f"sqg_inst_{t}_{r}.cu" for t in ("f32", "f64") for r in "abc"]
+SRCS = [os.path.join(CSRC, f) for f in ["sqg_capi.cu"] + _INST + ["closure_conv.cu", "closure_ops.cu"]]
 # headers each unit includes (a change rebuilds the unit)
+_PASS_HDRS = ["pdl.cuh", "sqg_fft.cuh", "sqg_kernels.cuh", "sqg_launch.cuh"]
 DEPS = {
-    "sqg_capi.cu": ["pdl.cuh", "sqg_fft.cuh", "sqg_kernels.cuh", "sqg_aux.cuh", "../../include/sqg.h"],
+    "sqg_capi.cu": _PASS_HDRS + ["sqg_aux.cuh", "../../include/sqg.h"],
     "closure_conv.cu": ["pdl.cuh", "closure_act.cuh", "../../include/sqg_closure.h"],
     "closure_ops.cu": ["pdl.cuh", "closure_act.cuh", "../../include/sqg_closure.h"],
 }
+DEPS.update({f: _PASS_HDRS for f in _INST})
 OUT = os.path.join(HERE, "libsqg.so")
 OBJ_DIR = os.path.join(HERE, "_build")
 
@@ -75,16 +78,20 @@ def build(force: bool = False, verbose: bool = False) -> str:
 def _build(force: bool, verbose: bool) -> str:
     t_start = time.time()
     os.makedirs(OBJ_DIR, exist_ok=True)
-    objs = []
+    objs, jobs = [], []
     for s in SRCS:
         o = _obj(s)
         if force or _stale(o, _deps(s)):
             cmd = [nvcc()] + NVCC_FLAGS + ["-c", "-o", o + ".tmp", s]
             if verbose:
                 print(" ".join(cmd))
-            subprocess.run(cmd, check=True)
-            os.replace(o + ".tmp", o)
+            jobs.append((o, subprocess.Popen(cmd)))
         objs.append(o)
+    failed = [o for o, pr in jobs if pr.wait() != 0]  # the units compile in parallel
+    if failed:
+        raise subprocess.CalledProcessError(1, "nvcc", output=f"failed: {failed}")
+    for o, _ in jobs:
+        os.replace(o + ".tmp", o)
     cmd = [nvcc()] + ARCH + ["-shared", "-o", OUT + ".tmp"] + objs
     if verbose:
         print(" ".join(cmd))

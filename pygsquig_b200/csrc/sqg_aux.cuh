@@ -6,6 +6,14 @@
 #include "sqg_kernels.cuh"
 
 namespace sqg {
+// Points the graph-replayed ring-phase control block at a phase table.
+__global__ void k_set_ctl(RingCtl* ctl, const double* base) {
+  ctl->base = base;
+  ctl->ctr = 0;
+}
+}  // namespace sqg
+
+namespace sqg {
 
 // out = L * theta, L = -mu [|k| < kf/2] - nu k2^(p/2): the damping term of
 // CombinedDamping.__call__ (damping.py:75-92) or, with mu = 0, the solver's

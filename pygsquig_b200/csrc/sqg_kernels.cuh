@@ -885,12 +885,6 @@ __device__ void ring_reduce(const KP& kp, const ColArgs& a) {
 
 }  // namespace sqg
 
-namespace sqg {
-__global__ void k_set_ctl(RingCtl* ctl, const double* base) {
-  ctl->base = base;
-  ctl->ctr = 0;
-}
-}  // namespace sqg
 
 namespace sqg {
 // ---- kernels: one plan, or a batch of members (member = blockIdx.y) ----

@@ -1,0 +1,221 @@
+// sqg_launch.cuh -- launch shapes of the row and column passes and the
+// per-size launch functions.
+//
+// The launch functions are templates over the precision T and log2(N).  Their
+// definitions (which instantiate the pass kernels) are compiled only by the
+// translation units sqg_inst_*.cu, each for a range of sizes, so that the
+// kernel instantiations build in parallel; sqg_capi.cu sees the declarations
+// and dispatches on log2(N) at run time.
+#pragma once
+#include "sqg_kernels.cuh"
+
+namespace sqg {
+
+// ---- compile-time launch shapes ----
+// Radix of the group FFTs.  Column pass: 16 for float grids with N >= 2048
+// (groups of N/16 threads, one exchange pass fewer, two 256-thread blocks per
+// SM; measured at N = 4096: 370 -> 271 us per launch); row pass: 8 at those
+// sizes (radix 16 with two exchange buffers made the fused stage pass slower,
+// 384 -> 508 us, because its stage update walks 16 prefetched chunks per
+// thread).  Grids with 128 <= N <= 2048: radix-4 row pass (twice the threads
+// per transform at 64 registers in single precision, 128 in double; at
+// N <= 1024 the pass is one wave of blocks bound by each block's latency:
+// FP32 N = 1024 row passes 31 -> 20 us, FP64 52 -> 36 us; N = 2048 step
+// FP32 0.64 -> 0.57 ms, FP64 1.36 -> 1.19 ms; at N = 4096 it was slower,
+// 315 -> 357 us); the column pass stays radix 8 there (radix 4 took
+// 23 -> 30 us at N = 1024 in single precision, 34 -> 39 us in double).
+template <typename T, int L>
+constexpr int col_radix() { return (sizeof(T) == 4 && L >= 11) ? 16 : 8; }
+template <typename T, int L>
+constexpr int row_radix() { return (L >= 7 && L <= 11) ? 4 : 8; }
+template <typename T, int L>
+constexpr int row_group() { return (1 << L) / row_radix<T, L>(); }
+template <typename T, int L>
+constexpr int col_group() { return (1 << L) / col_radix<T, L>(); }
+template <typename T, int L>
+constexpr int rows_per_cta() { return row_group<T, L>() >= 128 ? 1 : 128 / row_group<T, L>(); }
+template <typename T, int L>
+constexpr int pairs_per_cta() {
+  constexpr int g = col_group<T, L>();
+  constexpr int cap = (1 << L) / 2 < 16 ? (1 << L) / 2 : 16;
+  // radix 16: up to two column pairs (four columns fill the 32-byte sectors
+  // of each row's gather); the autotuner picks one or two
+  if (col_radix<T, L>() == 16) return 2;
+  return g >= 256 ? 1 : (256 / g > cap ? cap : 256 / g);
+}
+// Four resident field buffers per column pair when they fit in 150 KB; the
+// radix-16 column pass (FP32, N >= 2048) keeps two (two rounds of two fields,
+// about 35 KB a buffer: one or two column pairs per block as the autotuner
+// chose, 70 or 140 KB).
+template <typename T, int L>
+constexpr int col_nbuf() {
+  return col_radix<T, L>() == 16 ? 2
+         : (size_t)pairs_per_cta<T, L>() * 4 * ColBuf<(1 << L), col_radix<T, L>()>::SZ *
+                       sizeof(typename Cplx<T>::type) <= 150 * 1024 ? 4 : 2;
+}
+// Exchange buffers of the row pass: four (the theta fields transform
+// together) when they fit in 150 KB, else two (two rounds); two for a
+// radix-4 or radix-16 row pass.
+template <typename T, int L>
+constexpr int row_nfx() {
+  return row_radix<T, L>() != 8 ? 2
+         : (size_t)rows_per_cta<T, L>() * 4 * spad_size<row_radix<T, L>()>(1 << L) * sizeof(typename Cplx<T>::type) <=
+                   150 * 1024 ? 4 : 2;
+}
+template <typename T, int L>
+constexpr size_t row_base_smem() {
+  return (size_t)rows_per_cta<T, L>() * row_nfx<T, L>() * spad_size<row_radix<T, L>()>(1 << L) *
+         sizeof(typename Cplx<T>::type);
+}
+template <typename T, int L>
+constexpr size_t row_pf_bytes(int depth) {
+  return (size_t)rows_per_cta<T, L>() * depth * 4 * row_group<T, L>() * sizeof(typename Cplx<T>::type);
+}
+// Prefetch depth of the row pass: among R, R/2, R/4 and 1 chunks, the one
+// that lets the most blocks share an SM (the register budget's block count,
+// 227 KB of shared memory per SM with 1 KB reserved per block, at most 220 KB
+// per block), the deepest among equals: occupancy first, then prefetch depth.
+template <typename T, int L>
+constexpr int row_occupancy(int depth) {
+  constexpr int by_regs = min_blocks_r<T, row_radix<T, L>()>(rows_per_cta<T, L>() * row_group<T, L>());
+  const size_t smem = row_base_smem<T, L>() + row_pf_bytes<T, L>(depth);
+  if (smem > 220 * 1024) return 0;
+  const int by_smem = (int)((227 * 1024) / (smem + 1024));
+  return by_smem < by_regs ? by_smem : by_regs;
+}
+template <typename T, int L>
+constexpr int row_depth() {
+  constexpr int R = row_radix<T, L>();
+  int best = 1, occ = row_occupancy<T, L>(1);
+  for (int d = 2; d <= R; d *= 2) {
+    const int o = row_occupancy<T, L>(d);
+    if (o >= occ && o > 0) { occ = o; best = d; }
+  }
+  return best;
+}
+template <typename T, int L>
+size_t row_smem() { return row_base_smem<T, L>() + row_pf_bytes<T, L>(row_depth<T, L>()); }
+// The stage pass without inverse transforms (the last stage of a step): one
+// exchange buffer per row pair, registers as row_min_blocks<.., 1>; prefetch
+// depth again occupancy first.
+template <typename T, int L>
+constexpr size_t rowx_smem(int depth) {
+  return (size_t)rows_per_cta<T, L>() * spad_size<row_radix<T, L>()>(1 << L) * sizeof(typename Cplx<T>::type) +
+         row_pf_bytes<T, L>(depth);
+}
+template <typename T, int L>
+constexpr int rowx_occupancy(int depth) {
+  constexpr int by_regs = row_min_blocks<T, row_radix<T, L>(), 1>(rows_per_cta<T, L>() * row_group<T, L>());
+  const size_t smem = rowx_smem<T, L>(depth);
+  if (smem > 220 * 1024) return 0;
+  const int by_smem = (int)((227 * 1024) / (smem + 1024));
+  return by_smem < by_regs ? by_smem : by_regs;
+}
+template <typename T, int L>
+constexpr int rowx_depth() {
+  constexpr int R = row_radix<T, L>();
+  int best = 1, occ = rowx_occupancy<T, L>(1);
+  for (int d = 2; d <= R; d *= 2) {
+    const int o = rowx_occupancy<T, L>(d);
+    if (o >= occ && o > 0) { occ = o; best = d; }
+  }
+  return best;
+}
+template <typename T, int L>
+size_t col_smem() {  // per column pair: NBUF buffers plus the slack of col_qstride
+  return (size_t)pairs_per_cta<T, L>() *
+         (col_nbuf<T, L>() * ColBuf<(1 << L), col_radix<T, L>()>::SZ + line_elems<T>()) *
+         sizeof(typename Cplx<T>::type);
+}
+
+
+template <typename T, int L> cudaError_t launch_row_t(const KP& kp, const RowArgs& a, cudaStream_t st);
+template <typename T, int L> cudaError_t launch_col_t(const KP& kp, const ColArgs& a, cudaStream_t st, bool ring_only);
+template <typename T, int L> cudaError_t shape_max_t(int* rpc, int* np);
+template <typename T, int L> cudaError_t set_attrs_t();
+template <typename T, int L> cudaError_t launch_row_batch_t(const KP* kps, const RowArgs* as, int members, cudaStream_t st);
+template <typename T, int L> cudaError_t launch_col_batch_t(const KP* kps, const ColArgs* as, int members, cudaStream_t st);
+template <typename T, int L> cudaError_t set_batch_attrs_t();
+
+#ifdef SQG_LAUNCH_DEFS
+// Launch shapes: a.rpc row pairs per CTA of the row pass (a.np column pairs
+// per CTA of the column pass), a power-of-two divisor of the compiled maximum;
+// shared memory scales with it.  Results do not depend on the shape (every
+// row and column transform is computed the same way); only the number and
+// size of the CTAs change.
+// The row and column passes are launched with programmatic dependent launch
+// (pdl.cuh): the next pass's launch overlaps the tail of the current one.
+template <typename T, int L>
+cudaError_t launch_row_t(const KP& kp, const RowArgs& a, cudaStream_t st) {
+  constexpr int N = 1 << L, RPC = rows_per_cta<T, L>();
+  const int rpc = a.rpc > 0 ? a.rpc : RPC;
+  const int grid = (N / 2 + 1 + rpc - 1) / rpc;
+  if (a.rmode == RM_STAGE && !a.do_p1)
+    return launch_pdl(k_row<T, L, row_radix<T, L>(), RPC, rowx_depth<T, L>(), 1>, dim3(grid),
+                      dim3(rpc * row_group<T, L>()), rowx_smem<T, L>(rowx_depth<T, L>()) / RPC * rpc, st, kp, a);
+  return launch_pdl(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>, dim3(grid),
+                    dim3(rpc * row_group<T, L>()), row_smem<T, L>() / RPC * rpc, st, kp, a);
+}
+template <typename T, int L>
+cudaError_t launch_col_t(const KP& kp, const ColArgs& a, cudaStream_t st, bool ring_only) {
+  constexpr int N = 1 << L, NP = pairs_per_cta<T, L>();
+  const int np = a.np > 0 ? a.np : NP;
+  int grid = ring_only ? 1 : N / (2 * np) + (a.ring_cta ? 1 : 0);
+  return launch_pdl(k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()>, dim3(grid), dim3(np * col_group<T, L>()),
+                    col_smem<T, L>() / NP * np, st, kp, a);
+}
+template <typename T, int L>
+cudaError_t shape_max_t(int* rpc, int* np) {
+  *rpc = rows_per_cta<T, L>();
+  *np = pairs_per_cta<T, L>();
+  return cudaSuccess;
+}
+template <typename T, int L>
+cudaError_t set_attrs_t() {
+  constexpr int RPC = rows_per_cta<T, L>(), NP = pairs_per_cta<T, L>();
+  cudaError_t e = cudaFuncSetAttribute(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem<T, L>());
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_row<T, L, row_radix<T, L>(), RPC, rowx_depth<T, L>(), 1>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rowx_smem<T, L>(rowx_depth<T, L>()));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem<T, L>());
+}
+
+template <typename T, int L>
+cudaError_t launch_row_batch_t(const KP* kps, const RowArgs* as, int members, cudaStream_t st) {
+  constexpr int N = 1 << L, RPC = rows_per_cta<T, L>();
+  dim3 grid((N / 2 + 1 + RPC - 1) / RPC, members);
+  return launch_pdl(k_row_batch<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>, grid,
+                    dim3(RPC * row_group<T, L>()), row_smem<T, L>(), st, kps, as);
+}
+template <typename T, int L>
+cudaError_t launch_col_batch_t(const KP* kps, const ColArgs* as, int members, cudaStream_t st) {
+  constexpr int N = 1 << L, NP = pairs_per_cta<T, L>();
+  dim3 grid(N / (2 * NP), members);
+  return launch_pdl(k_col_batch<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()>, grid,
+                    dim3(NP * col_group<T, L>()), col_smem<T, L>(), st, kps, as);
+}
+template <typename T, int L>
+cudaError_t set_batch_attrs_t() {
+  constexpr int RPC = rows_per_cta<T, L>(), NP = pairs_per_cta<T, L>();
+  cudaError_t e = cudaFuncSetAttribute(k_row_batch<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem<T, L>());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_col_batch<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem<T, L>());
+}
+
+// Explicit instantiation of every launch function for one (T, log2 N).
+#define SQG_INSTANTIATE(T, L)                                                                               \
+  template cudaError_t launch_row_t<T, L>(const KP&, const RowArgs&, cudaStream_t);                        \
+  template cudaError_t launch_col_t<T, L>(const KP&, const ColArgs&, cudaStream_t, bool);                  \
+  template cudaError_t shape_max_t<T, L>(int*, int*);                                                      \
+  template cudaError_t set_attrs_t<T, L>();                                                                \
+  template cudaError_t launch_row_batch_t<T, L>(const KP*, const RowArgs*, int, cudaStream_t);             \
+  template cudaError_t launch_col_batch_t<T, L>(const KP*, const ColArgs*, int, cudaStream_t);             \
+  template cudaError_t set_batch_attrs_t<T, L>();
+#endif
+
+}  // namespace sqg
