@@ -268,10 +268,18 @@ int sqg_check_status(sqg_plan* plan, uint32_t* flags, void* stream);
 int sqg_last_launch_count(const sqg_plan* plan, int64_t* launches);
 
 /* Per-launch timing with CUDA events on the launching stream (instrumentation
- * for benchmarks; multistep then runs without its CUDA graph).
- * sqg_timing_read synchronises, returns total milliseconds and launch counts
- * per kind (0 row inverse pass, 1 row stage pass, 2 column pass, 3 scalar row
- * pass, 4 scalar column pass, 5 other) and clears the record. */
+ * for benchmarks; multistep then runs without its CUDA graph).  enable = 0
+ * off, 1 one event pair around every launch, k > 1 every launch site issues
+ * its pass k times back to back inside one event pair (the passes chained by
+ * programmatic dependent launch as inside a step; the results of such a call
+ * are not valid -- RK accumulators are updated k times -- and the next step
+ * recomputes every buffer from its inputs; refused for OU ring forcing,
+ * whose state the repeats would advance).  sqg_timing_read synchronises,
+ * returns total milliseconds and launch counts per kind (0 theta row inverse
+ * pass, 1 theta row stage pass with transforms, 2 theta column pass, 3 scalar
+ * row stage pass, 4 scalar column pass, 5 other, 6 theta row stage pass
+ * without transforms (last stage), 7 velocity row pass, 8 velocity column
+ * pass, 9 scalar row inverse pass) and clears the record. */
 int sqg_set_timing(sqg_plan* plan, int32_t enable);
 int sqg_timing_read(sqg_plan* plan, double* ms, int64_t* count, int32_t nkinds);
 

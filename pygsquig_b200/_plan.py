@@ -298,10 +298,14 @@ class Plan:
         _lib.check(self._lib.sqg_check_status(self._h, C.byref(f), _stream_ptr()))
         return int(f.value)
 
-    TIMING_KINDS = ("row_inverse", "row_stage", "col_theta", "row_scalar", "col_scalar", "other")
+    TIMING_KINDS = ("row_inverse", "row_stage", "col_theta", "row_scalar", "col_scalar", "other", "row_last",
+                    "row_vel", "col_vel", "row_scalar_inverse")
 
-    def set_timing(self, on: bool) -> None:
-        _lib.check(self._lib.sqg_set_timing(self._h, 1 if on else 0))
+    def set_timing(self, on, reps: int = 1) -> None:
+        """on=False: off.  on=True: events around every launch site, each site
+        issuing ``reps`` launches of its pass back to back (reps > 1: the
+        results of the timed calls are not valid)."""
+        _lib.check(self._lib.sqg_set_timing(self._h, (max(int(reps), 1)) if on else 0))
 
     def timing_read(self) -> dict:
         n = len(self.TIMING_KINDS)

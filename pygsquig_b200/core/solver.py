@@ -171,6 +171,7 @@ class gSQGSolver:
         """One RK4 step (solver.py:182-214)."""
         damp, ring, phases_key, generic = self._classify(forcing, damping, kwargs)
         pl = self.plan(damp, ring)
+        self._step_plan = pl  # the scalar stages of the same step run on this plan
         th = pl.check_spectrum(state["theta_hat"])
         phases = pl.phases_tensor(phases_key) if ring is not None else None
         out = torch.empty_like(th)

@@ -74,7 +74,9 @@ class gSQGSolverWithScalars(gSQGSolver):
         base = {k: v for k, v in state.items() if k != "scalar_state"}
         new = super().step(base, dt, forcing, damping, **kwargs)
         if self.species:
-            pl = self.plan()
+            # the plan the theta step just used (its scalar buffers serve the
+            # scalar stages; ring and damping do not enter them)
+            pl = self.__dict__.get("_step_plan") or self.plan()
             names = list(self.species)
             s_in = [pl.check_spectrum(ss.scalars[n], n) for n in names]
             s_out = [torch.empty_like(t) for t in s_in]

@@ -67,8 +67,9 @@ struct sqg_plan {
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   // per-launch CUDA-event timing (bench instrumentation)
   bool timing = false;
+  int timing_reps = 1;  // launches per launch site while timing
   std::vector<cudaEvent_t> ev_pool;
-  struct Rec { int kind; cudaEvent_t a, b; };
+  struct Rec { int kind; cudaEvent_t a, b; int reps; };
   std::vector<Rec> recs;
   size_t ev_used = 0;
 };
@@ -280,7 +281,7 @@ cudaError_t shape_max_p(int log2n, int* rpc, int* np) {
 
 // Timing kinds reported by sqg_timing_read.
 enum { TK_ROW_P1 = 0, TK_ROW_STAGE = 1, TK_COL_THETA = 2, TK_ROW_SCALAR = 3, TK_COL_SCALAR = 4, TK_OTHER = 5,
-       TK_COUNT = 6 };
+       TK_ROW_LAST = 6, TK_ROW_VEL = 7, TK_COL_VEL = 8, TK_ROW_SCALAR_P1 = 9, TK_COUNT = 10 };
 
 cudaEvent_t next_event(sqg_plan* pl) {
   if (pl->ev_used == pl->ev_pool.size()) {
@@ -291,27 +292,41 @@ cudaEvent_t next_event(sqg_plan* pl) {
   return pl->ev_pool[pl->ev_used++];
 }
 
+// With timing on, each launch site issues pl->timing_reps launches of its
+// pass back to back (the programmatic dependent launch between them as
+// between the passes of a step) inside one pair of events.
 template <typename F>
 cudaError_t timed(sqg_plan* pl, int kind, cudaStream_t st, F&& f) {
   pl->launches++;
   if (!pl->timing) return f();
   cudaEvent_t a = next_event(pl), b = next_event(pl);
   cudaEventRecord(a, st);
-  cudaError_t e = f();
+  cudaError_t e = cudaSuccess;
+  for (int r = 0; r < pl->timing_reps && e == cudaSuccess; ++r) e = f();
   cudaEventRecord(b, st);
-  pl->recs.push_back({kind, a, b});
+  pl->recs.push_back({kind, a, b, pl->timing_reps});
   return e;
 }
 
+int row_kind(const RowArgs& a) {
+  if (a.fmode == FM_SCAL) return a.rmode == RM_P1 ? TK_ROW_SCALAR_P1 : TK_ROW_SCALAR;
+  if (a.fmode == FM_VEL) return TK_ROW_VEL;
+  if (a.fmode != FM_THETA) return TK_OTHER;
+  if (a.rmode == RM_P1) return TK_ROW_P1;
+  if (a.rmode == RM_STAGE) return a.do_p1 ? TK_ROW_STAGE : TK_ROW_LAST;
+  return TK_OTHER;
+}
+
 cudaError_t launch_row(sqg_plan* pl, const KP& kp, const RowArgs& a, cudaStream_t st) {
-  const int kind = a.fmode == FM_SCAL ? TK_ROW_SCALAR : (a.rmode == RM_P1 ? TK_ROW_P1 : (a.rmode == RM_STAGE ? TK_ROW_STAGE : TK_OTHER));
+  const int kind = row_kind(a);
   return timed(pl, kind, st, [&] {
     return pl->d.precision == SQG_F64 ? launch_row_p<double>(pl->log2N, kp, a, st)
                                       : launch_row_p<float>(pl->log2N, kp, a, st);
   });
 }
 cudaError_t launch_col(sqg_plan* pl, const KP& kp, const ColArgs& a, cudaStream_t st, bool ring_only = false) {
-  const int kind = a.cmode == CM_THETA ? TK_COL_THETA : (a.cmode == CM_SCAL ? TK_COL_SCALAR : TK_OTHER);
+  const int kind = a.cmode == CM_THETA ? TK_COL_THETA
+                   : (a.cmode == CM_SCAL ? TK_COL_SCALAR : (a.cmode == CM_VEL ? TK_COL_VEL : TK_OTHER));
   return timed(pl, kind, st, [&] {
     return pl->d.precision == SQG_F64 ? launch_col_p<double>(pl->log2N, kp, a, st, ring_only)
                                       : launch_col_p<float>(pl->log2N, kp, a, st, ring_only);
@@ -1123,7 +1138,11 @@ int sqg_check_status(sqg_plan* pl, uint32_t* flags, void* stream) {
 
 int sqg_set_timing(sqg_plan* pl, int32_t enable) {
   if (!pl) return fail(SQG_ERR_INVALID, "null plan");
+  if (enable < 0) return fail(SQG_ERR_INVALID, "enable must be >= 0");
+  if (enable > 1 && pl->d.has_ring && pl->d.ring_tau_f > 0)
+    return fail(SQG_ERR_INVALID, "repeated timing launches would advance the forcing's OU state");
   pl->timing = enable != 0;
+  pl->timing_reps = enable > 1 ? enable : 1;
   pl->recs.clear();
   pl->ev_used = 0;
   return SQG_OK;
@@ -1136,7 +1155,7 @@ int sqg_timing_read(sqg_plan* pl, double* ms, int64_t* count, int32_t nkinds) {
     SQG_CUDA(cudaEventSynchronize(r.b));
     float t = 0.f;
     SQG_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
-    if (r.kind < nkinds) { ms[r.kind] += t; count[r.kind] += 1; }
+    if (r.kind < nkinds) { ms[r.kind] += t; count[r.kind] += r.reps; }
   }
   pl->recs.clear();
   pl->ev_used = 0;
