@@ -79,7 +79,8 @@ typedef struct sqg_plan sqg_plan;
 /* Buffers inside the workspace that the host may view (sqg_plan_buffer). */
 typedef enum {
   SQG_BUF_STAGE = 0,      /* N x N complex: stage input theta_s of the last stage */
-  SQG_BUF_UV = 1,         /* N x N complex: u + i v (physical) at the new time */
+  SQG_BUF_UV = 1,         /* N x N complex u + i v (physical) at the new time, column-pair-major:
+                             (x, y) at element ((y / 2) N + x) 2 + (y mod 2) */
   SQG_BUF_RING_FORCE = 2, /* n_ring complex128: ring forcing of the last stage (scaled) */
   SQG_BUF_STATUS = 3      /* uint32 status flags */
 } sqg_buffer;

@@ -562,6 +562,24 @@ struct ColArgs {
   int np;                   // column pairs per CTA (0: the compiled maximum NP)
 };
 
+// Velocity u + i v of the scalar passes in physical space, stored
+// column-pair-major: the complex (u, v) at (x, y) is element
+// ((y / 2) N + x) 2 + (y mod 2), so that a column pair's values for one x are
+// adjacent and consecutive x are consecutive (coalesced in the column pass).
+__device__ __forceinline__ size_t uv_index(int N, int x, int y) {
+  return (((size_t)(y >> 1) * N + x) << 1) + (y & 1);
+}
+__device__ __forceinline__ void store_pair(float2* p, float2 a, float2 b) {
+  *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ void store_pair(double2* p, double2 a, double2 b) { p[0] = a; p[1] = b; }
+__device__ __forceinline__ void load_pair(const float2* p, float2& a, float2& b) {
+  const float4 q = *reinterpret_cast<const float4*>(p);
+  a = make_float2(q.x, q.y);
+  b = make_float2(q.z, q.w);
+}
+__device__ __forceinline__ void load_pair(const double2* p, double2& a, double2& b) { a = p[0]; b = p[1]; }
+
 // Slots of one field buffer of a column group: the raw half columns
 // A[kx] = x(kx, ya) at slot kx and B[kx] = x(kx, ya + 1) at slot
 // col_offb + kx (kx = 0..N/2), later reused as the FFT exchange buffer.
@@ -657,6 +675,28 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
   const size_t fstride = (size_t)(H + 1) * N;
   C v[R];
 
+  if (a.cmode == CM_VEL && !a.out1) {
+    // u + i v for the scalar passes, column-pair-major (uv_index): both
+    // fields transformed together, one 16-byte (float) or two 16-byte
+    // (double) stores per thread and row
+    col_fetch<T, LOG2N, R, NP, NBUF>(xh, y0, 0, smem, np);
+    col_fetch<T, LOG2N, R, NP, NBUF>(xh + fstride, y0, 1, smem, np);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    C V[2][R];
+    col_first_load<T, LOG2N, R>(gbuf, j, V[0]);
+    col_first_load<T, LOG2N, R>(gbuf + SZ, j, V[1]);
+    fft_multi<T, LOG2N, R, +1, 2>(V, gbuf, SZ, j, tw);
+    C* o = reinterpret_cast<C*>(a.out0);
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+      const int x = j + m * G;
+      // V[f][m] = f(x, ya) + i f(x, ya + 1) for f = u, v
+      store_pair(o + uv_index(N, x, ya), mkc<C>(V[0][m].x, V[1][m].x), mkc<C>(V[0][m].y, V[1][m].y));
+    }
+    return;
+  }
   if (a.cmode == CM_VEL || a.cmode == CM_PHYS1) {
     const int nf = a.cmode == CM_VEL ? 2 : 1;
     for (int f = 0; f < nf; ++f) col_fetch<T, LOG2N, R, NP, NBUF>(xh + f * fstride, y0, f, smem, np);
@@ -758,12 +798,13 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
         }
       } else {
         // V0: s_x(a) + i s_x(b); V1: s_y(a) + i s_y(b); (u, v) from global
+        // (column-pair-major: one coalesced 16-byte load per row in float)
         const C* uvp = reinterpret_cast<const C*>(a.uv);
 #pragma unroll
         for (int m = 0; m < R; ++m) {
-          const size_t x = j + m * G;
-          const C w0 = uvp[x * N + ya];
-          const C w1 = uvp[x * N + ya + 1];
+          const int x = j + m * G;
+          C w0, w1;
+          load_pair(uvp + uv_index(N, x, ya), w0, w1);
           W[m].x = w0.x * V[0][m].x + w0.y * V[1][m].x;
           W[m].y = w1.x * V[0][m].y + w1.y * V[1][m].y;
         }
