@@ -63,6 +63,23 @@ template <int DIR, typename C> __device__ __forceinline__ C mul_i(C a) {
   return r;
 }
 
+// Single precision: the same operations on packed pairs (sm_100's two-lane
+// FP32 add, multiply and fused multiply-add issue one instruction for both
+// components; each lane rounds as the scalar operation does).
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
+// a * b = a.x (b.x, b.y) + a.y (-b.y, b.x)
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return __ffma2_rn(make_float2(a.y, a.y), make_float2(-b.y, b.x), __fmul2_rn(make_float2(a.x, a.x), b));
+}
+// a * conj(b) = a.x (b.x, -b.y) + a.y (b.y, b.x)
+template <bool CONJ> __device__ __forceinline__ float2 cmul_tw(float2 a, float2 b) {
+  if (CONJ)
+    return __ffma2_rn(make_float2(a.y, a.y), make_float2(b.y, b.x), __fmul2_rn(make_float2(a.x, a.x), make_float2(b.x, -b.y)));
+  return cmul(a, b);
+}
+
 template <int DIR, typename C>
 __device__ __forceinline__ void dft2(C& a0, C& a1) {
   C t = a0; a0 = cadd(t, a1); a1 = csub(t, a1);
@@ -84,12 +101,10 @@ __device__ __forceinline__ void dft8s(C* v, int o, int st) {
   dft4<DIR>(e0, e1, e2, e3);
   dft4<DIR>(o0, o1, o2, o3);
   const T r = (T)0.70710678118654752440;  // 1/sqrt(2)
-  C t1, t3;
-  // o1 * (1 + DIR i)/sqrt2
-  t1.x = (o1.x - (T)DIR * o1.y) * r; t1.y = (o1.y + (T)DIR * o1.x) * r;
+  // t1 = o1 (1 + DIR i)/sqrt2 = (o1 + DIR i o1) r;  t3 = o3 (-1 + DIR i)/sqrt2
+  const C t1 = cscale(cadd(o1, mul_i<DIR>(o1)), r);
   C t2 = mul_i<DIR>(o2);
-  // o3 * (-1 + DIR i)/sqrt2
-  t3.x = (-o3.x - (T)DIR * o3.y) * r; t3.y = (-o3.y + (T)DIR * o3.x) * r;
+  const C t3 = cscale(csub(mul_i<DIR>(o3), o3), r);
   v[o] = cadd(e0, o0); v[o + 4 * st] = csub(e0, o0);
   v[o + st] = cadd(e1, t1); v[o + 5 * st] = csub(e1, t1);
   v[o + 2 * st] = cadd(e2, t2); v[o + 6 * st] = csub(e2, t2);
@@ -106,11 +121,15 @@ __device__ __forceinline__ void dft16(C (&v)[16]) {
 #pragma unroll
   for (int k = 0; k < 4; ++k) dft4<DIR>(v[k], v[k + 4], v[k + 8], v[k + 12]);
   // v[k + 4 m] now holds X_k[m]; multiply by w16^(k m), w16 = exp(DIR 2 pi i / 16)
-  auto rot = [&](C a, T c, T s) {  // a * (c + DIR i s)
-    C r;
-    r.x = a.x * c - (T)DIR * a.y * s;
-    r.y = a.y * c + (T)DIR * a.x * s;
-    return r;
+  auto rot = [&](C a, T c, T s) {  // a * (c + DIR i s) = a c + (DIR i a) s
+    if constexpr (sizeof(T) == 4) {
+      return __ffma2_rn(mul_i<DIR>(a), make_float2(s, s), __fmul2_rn(a, make_float2(c, c)));
+    } else {
+      C r;
+      r.x = a.x * c - (T)DIR * a.y * s;
+      r.y = a.y * c + (T)DIR * a.x * s;
+      return r;
+    }
   };
   v[5] = rot(v[5], c1, s1);    // k=1 m=1: w^1
   v[9] = rot(v[9], h, h);      // k=1 m=2: w^2

@@ -580,49 +580,40 @@ __device__ __forceinline__ void load_pair(const float2* p, float2& a, float2& b)
 }
 __device__ __forceinline__ void load_pair(const double2* p, double2& a, double2& b) { a = p[0]; b = p[1]; }
 
-// Slots of one field buffer of a column group: the raw half columns
-// A[kx] = x(kx, ya) at slot kx and B[kx] = x(kx, ya + 1) at slot
-// col_offb + kx (kx = 0..N/2), later reused as the FFT exchange buffer.
-template <int N, int R> struct ColBuf { static constexpr int SZ = spad_size<R>(N) + 2; };
+// Slots of one field buffer of a column group: the raw half columns of the
+// pair, interleaved by row -- slot 2 kx = x(kx, ya), slot 2 kx + 1 =
+// x(kx, ya + 1) for kx = 0..N/2 -- later reused as the FFT exchange buffer.
+// SZ is even, so every buffer starts on a 16-byte boundary.
+template <int N, int R> struct ColBuf { static constexpr int SZ = (spad_size<R>(N) + 2 + 1) & ~1; };
 
-// Placement of the raw half columns, chosen for the cp.async writes of
-// col_fetch: consecutive threads write (column pair q, half b, row kx) with
-// (q, b) fastest, so the 16 eight-byte writes of a half-warp (8 sixteen-byte
-// writes of a quarter-warp in double) span 2 np groups of rows.  B starts L/2
-// slots past a multiple of the line (L = elements per 128-byte line) and the
-// buffers of pair q start q * col_qstride(np), with col_qstride = L / (2 np)
-// modulo L, so the groups fill distinct banks (placed at H + 1 and
-// q * NBUF * SZ they took two to four shared-memory wavefronts per ideal one).
-// Each pair's buffers carry L slack slots for the stride adjustment.
-template <typename T> __host__ __device__ constexpr int line_elems() {
-  return 128 / (int)sizeof(typename Cplx<T>::type);
-}
-template <typename T, int N, int R> __host__ __device__ constexpr int col_offb() {
-  constexpr int L = line_elems<T>(), H = N / 2;
-  constexpr int off = H + 1 + ((L / 2 - (H + 1)) % L + L) % L;
-  return off + H + 1 <= ColBuf<N, R>::SZ ? off : H + 1;
-}
-template <typename T, int N, int R, int NBUF> __device__ __forceinline__ int col_qstride(int np) {
-  constexpr int L = line_elems<T>(), base = NBUF * ColBuf<N, R>::SZ;
-  const int want = 2 * np <= L ? L / (2 * np) : 1;
-  return base + ((want - base) % L + L) % L;
+// 16-byte asynchronous global -> shared copy (both addresses 16-byte aligned).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
 // Issue the copies of the half columns of field f for every column pair of
 // the block into buffer slot `buf` of each group (no registers, no wait).
+// A row of a column pair is 2 sizeof(C) contiguous bytes (one 16-byte copy in
+// float, two in double).  Copy unit u = (row kx, pair q, part): part fastest,
+// then the pair, so consecutive threads read a row's 16 np contiguous bytes
+// and write consecutive 16-byte slots (shifts only: np is a power of two).
 template <typename T, int LOG2N, int R, int NP, int NBUF>
 __device__ __forceinline__ void col_fetch(const typename Cplx<T>::type* __restrict__ f, int y0, int buf,
                                           typename Cplx<T>::type* smem, int np) {
   using C = typename Cplx<T>::type;
-  constexpr int N = 1 << LOG2N, H = N / 2, SZ = ColBuf<N, R>::SZ, OFFB = col_offb<T, N, R>();
-  const int qs = col_qstride<T, N, R, NBUF>(np);
-  const int total = (H + 1) * np * 2;
-  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    const int c = idx % (2 * np);      // column within the block (fastest: coalesced rows)
-    const int kx = idx / (2 * np);
-    const int q = c >> 1, b = c & 1;
-    C* z = smem + (size_t)q * qs + (size_t)buf * SZ;
-    cp_async_elem(z + b * OFFB + kx, f + (size_t)kx * N + y0 + c, (int)sizeof(C));
+  constexpr int N = 1 << LOG2N, H = N / 2, SZ = ColBuf<N, R>::SZ;
+  constexpr int LC = sizeof(C) == 16 ? 1 : 0;  // log2(16-byte copies per row of a pair)
+  const int ls = LC + (31 - __clz(np));        // log2(copy units per row)
+  const int units = (H + 1) << ls;
+  unsigned char* zb = reinterpret_cast<unsigned char*>(smem + (size_t)buf * SZ);
+  const unsigned char* gb = reinterpret_cast<const unsigned char*>(f + y0);
+  for (int u = threadIdx.x; u < units; u += blockDim.x) {
+    const int part = u & ((1 << LC) - 1);
+    const int q = (u >> LC) & (np - 1);
+    const int kx = u >> ls;
+    cp_async16(zb + ((size_t)q * NBUF * SZ + 2 * kx) * sizeof(C) + part * 16,
+               gb + ((size_t)kx * N + 2 * q) * sizeof(C) + part * 16);
   }
 }
 
@@ -632,12 +623,13 @@ template <typename T, int LOG2N, int R>
 __device__ __forceinline__ void col_first_load(const typename Cplx<T>::type* z, int j,
                                                typename Cplx<T>::type (&v)[R]) {
   using C = typename Cplx<T>::type;
-  constexpr int N = 1 << LOG2N, H = N / 2, G = N / R, OFFB = col_offb<T, N, R>();
+  constexpr int N = 1 << LOG2N, H = N / 2, G = N / R;
 #pragma unroll
   for (int m = 0; m < R; ++m) {
     const int x = j + m * G;
     const int kx = x <= H ? x : N - x;
-    const C xa = z[kx], xb = z[OFFB + kx];
+    C xa, xb;
+    load_pair(z + 2 * kx, xa, xb);
     if (x == 0 || x == H) v[m] = mkc<C>(xa.x, xb.x);
     else if (x < H) v[m] = mkc<C>(xa.x - xb.y, xa.y + xb.x);
     else v[m] = mkc<C>(xa.x + xb.y, -xa.y + xb.x);
@@ -666,7 +658,7 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
   const int grp = threadIdx.x / G;
   const int j = threadIdx.x - grp * G;
   const int np = a.np > 0 ? a.np : NP;       // launch shape (autotuned), <= NP
-  const int qs = col_qstride<T, N, R, NBUF>(np);
+  constexpr int qs = NBUF * SZ;              // slots per column pair
   C* gbuf = smem + (size_t)grp * qs;         // this group's NBUF buffers
   const int y0 = blockIdx.x * (2 * np);
   const int ya = y0 + 2 * grp;
@@ -829,19 +821,18 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
   __syncthreads();
   // split: Ja(kx) = (W(kx) + conj W(-kx))/2, Jb(kx) = -i (W(kx) - conj W(-kx))/2
   C* jh = reinterpret_cast<C*>(a.jh);
-  const int total = (H + 1) * np;
+  const int lnp = 31 - __clz(np);  // np is a power of two
+  const int total = (H + 1) << lnp;
   for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    const int kx = idx / np;
-    const int q = idx - kx * np;
+    const int kx = idx >> lnp;
+    const int q = idx & (np - 1);
     const C* w = smem + (size_t)q * qs;
     const C wk = w[spad<R, T>(kx)];
     const C wm = w[spad<R, T>((N - kx) & (N - 1))];
     const C ja = mkc<C>((T)0.5 * (wk.x + wm.x), (T)0.5 * (wk.y - wm.y));
     const C d = mkc<C>(wk.x - wm.x, wk.y + wm.y);
     const C jb = mkc<C>((T)0.5 * d.y, (T)-0.5 * d.x);
-    const int y = y0 + 2 * q;
-    jh[(size_t)kx * N + y] = ja;
-    jh[(size_t)kx * N + y + 1] = jb;
+    store_pair(jh + (size_t)kx * N + y0 + 2 * q, ja, jb);
   }
 }
 

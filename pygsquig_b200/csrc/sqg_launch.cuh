@@ -122,9 +122,8 @@ constexpr int rowx_depth() {
   return best;
 }
 template <typename T, int L>
-size_t col_smem() {  // per column pair: NBUF buffers plus the slack of col_qstride
-  return (size_t)pairs_per_cta<T, L>() *
-         (col_nbuf<T, L>() * ColBuf<(1 << L), col_radix<T, L>()>::SZ + line_elems<T>()) *
+size_t col_smem() {  // per column pair: NBUF buffers
+  return (size_t)pairs_per_cta<T, L>() * col_nbuf<T, L>() * ColBuf<(1 << L), col_radix<T, L>()>::SZ *
          sizeof(typename Cplx<T>::type);
 }
 
