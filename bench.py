@@ -448,7 +448,7 @@ def main():
             dist.barrier()
         th = st["theta_hat"]
         finite = bool(torch.isfinite(torch.view_as_real(th)).all().item())
-        res = {"ms": ms, "steps": steps, "launches": launches, "finite": finite,
+        res = {"ms": ms, "steps": steps, "launches": launches, "finite": finite, "launch_shape": pl.shape(),
                "clocks": sampler.summary(t_wall0 - 0.1, time.time()) if sampler else None}
         # ---- per-pass durations: each launch site of one step issues its pass
         # TIMING_REPS times back to back inside one event pair (on a copy of the
@@ -661,6 +661,7 @@ def main():
                        "frac_of_peak": model_bytes / (ms_per_step / 1e3) / 1e9 / peak},
         "kernels": kern,
         "kernel_timing": ksum,
+        "launch_shape": main_res["launch_shape"],
         "gpu_launches": main_res["launches"],
         "clocks": main_res["clocks"],
         "e2e": main_res["e2e"],

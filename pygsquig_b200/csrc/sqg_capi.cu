@@ -658,12 +658,17 @@ int sqg_plan_autotune(sqg_plan* pl, int32_t reps, void* stream) {
   cudaEvent_t e0, e1;
   SQG_CUDA(cudaEventCreate(&e0));
   SQG_CUDA(cudaEventCreate(&e1));
-  float best = 1e30f;
-  int br = 0, bn = 0;
-  for (int r = mr; r >= 1 && rc == SQG_OK; r /= 2) {
-    for (int n = mn; n >= 1 && rc == SQG_OK; n /= 2) {
-      pl->rpc = r;
-      pl->np = n;
+  // every shape is timed in three interleaved rounds and keeps its fastest
+  // round, so that a clock ramp or a stray slow round early on does not
+  // decide the choice
+  std::vector<std::pair<int, int>> shapes;
+  for (int r = mr; r >= 1; r /= 2)
+    for (int n = mn; n >= 1; n /= 2) shapes.push_back({r, n});
+  std::vector<float> t_best(shapes.size(), 1e30f);
+  for (int round = 0; round < 3 && rc == SQG_OK; ++round) {
+    for (size_t i = 0; i < shapes.size() && rc == SQG_OK; ++i) {
+      pl->rpc = shapes[i].first;
+      pl->np = shapes[i].second;
       if ((rc = one()) != SQG_OK) break;  // warm-up
       cudaEventRecord(e0, st);
       for (int k = 0; k < reps && rc == SQG_OK; ++k) rc = one();
@@ -671,9 +676,13 @@ int sqg_plan_autotune(sqg_plan* pl, int32_t reps, void* stream) {
       if (cudaEventSynchronize(e1) != cudaSuccess) { rc = fail(SQG_ERR_CUDA, "autotune: event"); break; }
       float ms = 0.f;
       cudaEventElapsedTime(&ms, e0, e1);
-      if (ms < best) { best = ms; br = r; bn = n; }
+      if (ms < t_best[i]) t_best[i] = ms;
     }
   }
+  float best = 1e30f;
+  int br = mr, bn = mn;
+  for (size_t i = 0; i < shapes.size(); ++i)
+    if (t_best[i] < best) { best = t_best[i]; br = shapes[i].first; bn = shapes[i].second; }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   pl->timing = timing;

@@ -119,12 +119,17 @@ constexpr int min_blocks_r(int threads) {
                 : min_blocks<T>(threads);
 }
 
-// Row-pass blocks: the pass without the inverse transforms (NFX = 1) is held
-// to the radix-4 register budget (64 a thread in single precision, 128 in
-// double), so that more of its blocks fit than of the full pass.
+// Row-pass blocks: the pass without the inverse transforms (NFX = 0) and the
+// radix-8 pass that transforms one field at a time (NFX = 1) are held to the
+// radix-4 register budget (64 a thread in single precision, 128 in double),
+// so that more of their blocks fit than of the passes that transform several
+// fields together; the radix-16 one-field pass (256 threads) gets 128
+// registers in single precision, two blocks per SM.
 template <typename T, int R, int NFX>
 constexpr int row_min_blocks(int threads) {
-  return NFX == 1 ? min_blocks_r<T, 4>(threads) : min_blocks_r<T, R>(threads);
+  // radix 16 one field at a time: 128 registers (two 256-thread blocks per SM)
+  return (NFX == 1 && R == 16) ? min_blocks<T>(threads)
+                               : (NFX <= 1 ? min_blocks_r<T, 4>(threads) : min_blocks_r<T, R>(threads));
 }
 
 __device__ __forceinline__ int mode_abs(int i, int N) { return i <= (N >> 1) ? i : N - i; }
@@ -190,11 +195,9 @@ __device__ __forceinline__ int field_kind(int fmode, int f) {
 
 // Fields f0 .. f0+NF-1 of the row pair's mode: form their spectra from
 // theta_{s+1} at (p, iy) / (N-p, N-iy), transform them together along y and
-// write xh[f][p][:].  Also writes the mean-gradient source spectra of the
-// scalars when asked (needs u and v in the same batch).
-template <typename T, int LOG2N, int R, int NF>
-__device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, const typename Cplx<T>::type (&t1)[R],
-                                           const typename Cplx<T>::type (&t2)[R], int f0, int j, int p, bool valid,
+// write xh[f][p][:].
+template <typename T, int LOG2N, int R, int NF, typename HA>
+__device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, HA ha, int f0, int j, int p, bool valid,
                                            typename Cplx<T>::type* wbuf) {
   using C = typename Cplx<T>::type;
   constexpr int N = 1 << LOG2N, G = N / R, H = N / 2, XB = spad_size<R>(N);
@@ -208,8 +211,8 @@ __device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, const
 #pragma unroll
   for (int m = 0; m < R; ++m) {
     const int iy = j + m * G;
-    const C h = cscale(cadd(t1[m], cconj(t2[m])), (T)0.5);
-    const C an = cscale(csub(t1[m], cconj(t2[m])), (T)0.5);
+    C h, an;
+    ha(m, h, an);
     const T ky = (T)wavenumber(kp, iy);
     const T dky = (iy == H) ? (T)0 : ky;
     const T nky = (iy == H) ? ky : (T)0;
@@ -234,14 +237,17 @@ __device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, const
       }
       V[f][m] = X;
     }
-    if (NF >= 2 && uv && f0 == 0 && a.n_src > 0 && valid) {
-      // S^ = -N^2 (gx X_u + gy X_v): the mean-gradient scalar source
-      const T n2 = (T)1 / s_n2;
-      for (int sidx = 0; sidx < a.n_src; ++sidx) {
-        C* so = reinterpret_cast<C*>(a.src_out[sidx]);
-        const T gx = (T)a.gx[sidx], gy = (T)a.gy[sidx];
-        so[(size_t)p * N + iy] =
-            mkc<C>(-n2 * (gx * V[0][m].x + gy * V[1][m].x), -n2 * (gx * V[0][m].y + gy * V[1][m].y));
+    if constexpr (NF >= 2) {
+      if (uv && f0 == 0 && a.n_src > 0 && valid) {
+        // S^ = -N^2 (gx X_u + gy X_v): the mean-gradient scalar sources, from
+        // the u and v spectra of this batch
+        const T n2 = (T)1 / s_n2;
+        for (int sidx = 0; sidx < a.n_src; ++sidx) {
+          C* so = reinterpret_cast<C*>(a.src_out[sidx]);
+          const T gx = (T)a.gx[sidx], gy = (T)a.gy[sidx];
+          so[(size_t)p * N + iy] =
+              mkc<C>(-n2 * (gx * V[0][m].x + gy * V[1][m].x), -n2 * (gx * V[0][m].y + gy * V[1][m].y));
+        }
       }
     }
   }
@@ -253,6 +259,40 @@ __device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, const
     for (int f = 0; f < NF; ++f)
 #pragma unroll
       for (int m = 0; m < R; ++m) xh[(f0 + f) * fstride + (size_t)p * N + j + m * G] = V[f][m];
+  }
+}
+
+// Mean-gradient scalar sources S^ = -N^2 (gx X_u + gy X_v) = -(gx u^ + gy v^)
+// on rows p (kx >= 0) from the spectra X_u, X_v of the u and v fields (the
+// expressions of row_fields), for the n_src scalars that carry one; used by
+// the one-field-at-a-time pass, where u and v are not in the same batch.
+template <typename T, int LOG2N, int R, typename HA>
+__device__ __forceinline__ void row_sources(const KP& kp, const RowArgs& a, HA ha, int j, int p) {
+  using C = typename Cplx<T>::type;
+  constexpr int N = 1 << LOG2N, G = N / R, H = N / 2;
+  const T kx = (T)wavenumber(kp, p);
+  const T s_n2 = (T)kp.inv_n2;
+  const T dkx = (p == H) ? (T)0 : kx;
+  const T nkx = (p == H) ? kx : (T)0;
+  const T n2 = (T)1 / s_n2;
+#pragma unroll
+  for (int m = 0; m < R; ++m) {
+    const int iy = j + m * G;
+    C h, an;
+    ha(m, h, an);
+    const T ky = (T)wavenumber(kp, iy);
+    const T dky = (iy == H) ? (T)0 : ky;
+    const T nky = (iy == H) ? ky : (T)0;
+    const T mm = inv_frac<T>(kx * kx + ky * ky, (T)kp.alpha, kp.akind) * s_n2;
+    const C qu = cadd(cscale(h, dky), cscale(an, nky));
+    const C qv = cadd(cscale(h, dkx), cscale(an, nkx));
+    const C Xu = mkc<C>(mm * qu.y, -mm * qu.x);
+    const C Xv = mkc<C>(-mm * qv.y, mm * qv.x);
+    for (int sidx = 0; sidx < a.n_src; ++sidx) {
+      C* so = reinterpret_cast<C*>(a.src_out[sidx]);
+      const T gx = (T)a.gx[sidx], gy = (T)a.gy[sidx];
+      so[(size_t)p * N + iy] = mkc<C>(-n2 * (gx * Xu.x + gy * Xv.x), -n2 * (gx * Xu.y + gy * Xv.y));
+    }
   }
 }
 
@@ -271,10 +311,12 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a) {
   const int grp = threadIdx.x / G;
   const int j = threadIdx.x - grp * G;
   constexpr int XB = spad_size<R>(N);  // one exchange buffer
-  C* wbuf = smem + (size_t)grp * NFX * XB;  // NFX exchange buffers of this group
+  constexpr int NB = NFX > 0 ? NFX : 1;  // exchange buffers per group
+  C* wbuf = smem + (size_t)grp * NB * XB;
   // prefetch staging: DEPTH chunks x 4 slots (theta_n e1/e2, acc e1/e2) x G
   const int rpc = a.rpc > 0 ? a.rpc : RPC;  // launch shape (autotuned), <= RPC
-  C* pf = smem + (size_t)rpc * NFX * XB + (size_t)grp * (DEPTH * 4 * G);
+  C* pf = smem + (size_t)rpc * NB * XB + (size_t)grp * (DEPTH * 4 * G);
+  static_assert(NFX != 1 || DEPTH * 4 * G >= 2 * N, "the one-field pass keeps h and an in the staging slots");
   const int p_raw = blockIdx.x * rpc + grp;
   const bool valid = p_raw <= H;
   const int p = valid ? p_raw : H;
@@ -485,10 +527,10 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a) {
   if (kp.status) {
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(kp.status, 1u);
   }
-  // NFX = 1 is the instantiation for stage passes without the inverse
+  // NFX = 0 is the instantiation for stage passes without the inverse
   // transforms (the last stage of a step): compiled without them, it needs
   // few registers and one exchange buffer, so two blocks share an SM.
-  if constexpr (NFX < 2) {
+  if constexpr (NFX == 0) {
     return;
   } else {
   if (!a.do_p1) return;
@@ -507,19 +549,58 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a) {
       for (int m = 0; m < R; ++m) t2[m] = wbuf[(N - (j + m * G)) & (N - 1)];
     }
   }
-  // Inverse transforms along y of the multiplied Hermitian projections.
-  if (a.fmode == FM_THETA) {
-    if (NFX >= 4) {
-      row_fields<T, LOG2N, R, 4>(kp, a, t1, t2, 0, j, p, valid, wbuf);
-    } else {
-      row_fields<T, LOG2N, R, 2>(kp, a, t1, t2, 0, j, p, valid, wbuf);
-      row_fields<T, LOG2N, R, 2>(kp, a, t1, t2, 2, j, p, valid, wbuf);
+  // Hermitian and anti-Hermitian parts of theta_{s+1} at (p, iy), h = (t1 +
+  // conj t2) / 2 and an = (t1 - conj t2) / 2, for the transforms: from the
+  // registers, or -- in the one-field-at-a-time pass, which must fit in 64
+  // registers -- computed once into this group's prefetch staging slots
+  // (free once the update has consumed them; indices j + m G and N + j + m G
+  // are this thread's own slots, so no barrier is needed).
+  C* hs = pf;
+  if constexpr (NFX == 1) {
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+      hs[j + m * G] = cscale(cadd(t1[m], cconj(t2[m])), (T)0.5);
+      hs[N + j + m * G] = cscale(csub(t1[m], cconj(t2[m])), (T)0.5);
     }
-  } else if (a.fmode == FM_PHYS1) {
-    row_fields<T, LOG2N, R, 1>(kp, a, t1, t2, 0, j, p, valid, wbuf);
-  } else {
-    row_fields<T, LOG2N, R, 2>(kp, a, t1, t2, 0, j, p, valid, wbuf);
   }
+  auto ha_reg = [&](int m, C& h, C& an) {
+    h = cscale(cadd(t1[m], cconj(t2[m])), (T)0.5);
+    an = cscale(csub(t1[m], cconj(t2[m])), (T)0.5);
+  };
+  auto ha_smem = [&](int m, C& h, C& an) {
+    h = hs[j + m * G];
+    an = hs[N + j + m * G];
+  };
+  auto fields = [&](auto ha) {
+    // (the passes that transform u and v together write the sources there)
+    if constexpr (NFX == 1) {
+      if (a.fmode == FM_VEL && a.n_src > 0 && valid) row_sources<T, LOG2N, R>(kp, a, ha, j, p);
+    }
+    // Inverse transforms along y of the multiplied Hermitian projections,
+    // NFX fields at a time.
+    if (a.fmode == FM_THETA) {
+      if constexpr (NFX >= 4) {
+        row_fields<T, LOG2N, R, 4>(kp, a, ha, 0, j, p, valid, wbuf);
+      } else if constexpr (NFX == 2) {
+        row_fields<T, LOG2N, R, 2>(kp, a, ha, 0, j, p, valid, wbuf);
+        row_fields<T, LOG2N, R, 2>(kp, a, ha, 2, j, p, valid, wbuf);
+      } else {
+#pragma unroll 1
+        for (int f = 0; f < 4; ++f) row_fields<T, LOG2N, R, 1>(kp, a, ha, f, j, p, valid, wbuf);
+      }
+    } else if (a.fmode == FM_PHYS1) {
+      row_fields<T, LOG2N, R, 1>(kp, a, ha, 0, j, p, valid, wbuf);
+    } else {
+      if constexpr (NFX >= 2) {
+        row_fields<T, LOG2N, R, 2>(kp, a, ha, 0, j, p, valid, wbuf);
+      } else {
+#pragma unroll 1
+        for (int f = 0; f < 2; ++f) row_fields<T, LOG2N, R, 1>(kp, a, ha, f, j, p, valid, wbuf);
+      }
+    }
+  };
+  if constexpr (NFX == 1) fields(ha_smem);
+  else fields(ha_reg);
   }
 }
 

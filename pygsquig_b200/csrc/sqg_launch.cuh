@@ -28,6 +28,14 @@ template <typename T, int L>
 constexpr int col_radix() { return (sizeof(T) == 4 && L >= 11) ? 16 : 8; }
 template <typename T, int L>
 constexpr int row_radix() { return (L >= 7 && L <= 11) ? 4 : 8; }
+// The last stage of a step (no inverse transforms) uses the same radix, so
+// that a step and a replayed multistep step round identically.
+template <typename T, int L>
+constexpr int rowx_radix() { return row_radix<T, L>(); }
+template <typename T, int L>
+constexpr int rowx_group() { return (1 << L) / rowx_radix<T, L>(); }
+template <typename T, int L>
+constexpr int rowx_rpc() { return rowx_group<T, L>() >= 128 ? 1 : 128 / rowx_group<T, L>(); }
 template <typename T, int L>
 constexpr int row_group() { return (1 << L) / row_radix<T, L>(); }
 template <typename T, int L>
@@ -62,9 +70,15 @@ constexpr int row_nfx() {
          : (size_t)rows_per_cta<T, L>() * 4 * spad_size<row_radix<T, L>()>(1 << L) * sizeof(typename Cplx<T>::type) <=
                    150 * 1024 ? 4 : 2;
 }
+// Scalar stage passes (two fields: s_x, s_y) at N = 4096 in float transform
+// one field at a time at 64 registers, two 512-thread blocks per SM
+// (measured: 258 -> 222 us per launch; the theta passes with four fields
+// were slower that way, 354 -> 394 us, and keep row_nfx).
 template <typename T, int L>
+constexpr int row_nfx_scalar() { return (sizeof(T) == 4 && L == 12) ? 1 : row_nfx<T, L>(); }
+template <typename T, int L, int NFX = row_nfx<T, L>()>
 constexpr size_t row_base_smem() {
-  return (size_t)rows_per_cta<T, L>() * row_nfx<T, L>() * spad_size<row_radix<T, L>()>(1 << L) *
+  return (size_t)rows_per_cta<T, L>() * (NFX > 0 ? NFX : 1) * spad_size<row_radix<T, L>()>(1 << L) *
          sizeof(typename Cplx<T>::type);
 }
 template <typename T, int L>
@@ -75,37 +89,40 @@ constexpr size_t row_pf_bytes(int depth) {
 // that lets the most blocks share an SM (the register budget's block count,
 // 227 KB of shared memory per SM with 1 KB reserved per block, at most 220 KB
 // per block), the deepest among equals: occupancy first, then prefetch depth.
-template <typename T, int L>
+template <typename T, int L, int NFX = row_nfx<T, L>()>
 constexpr int row_occupancy(int depth) {
-  constexpr int by_regs = min_blocks_r<T, row_radix<T, L>()>(rows_per_cta<T, L>() * row_group<T, L>());
-  const size_t smem = row_base_smem<T, L>() + row_pf_bytes<T, L>(depth);
+  constexpr int by_regs = row_min_blocks<T, row_radix<T, L>(), NFX>(rows_per_cta<T, L>() * row_group<T, L>());
+  const size_t smem = row_base_smem<T, L, NFX>() + row_pf_bytes<T, L>(depth);
   if (smem > 220 * 1024) return 0;
   const int by_smem = (int)((227 * 1024) / (smem + 1024));
   return by_smem < by_regs ? by_smem : by_regs;
 }
-template <typename T, int L>
+template <typename T, int L, int NFX = row_nfx<T, L>()>
 constexpr int row_depth() {
   constexpr int R = row_radix<T, L>();
-  int best = 1, occ = row_occupancy<T, L>(1);
+  int best = 1, occ = row_occupancy<T, L, NFX>(1);
   for (int d = 2; d <= R; d *= 2) {
-    const int o = row_occupancy<T, L>(d);
+    const int o = row_occupancy<T, L, NFX>(d);
     if (o >= occ && o > 0) { occ = o; best = d; }
   }
+  // the one-field pass keeps h and an in the staging slots (2 N elements)
+  if (NFX == 1)
+    while (best < R && best * 4 * row_group<T, L>() < 2 * (1 << L)) best *= 2;
   return best;
 }
-template <typename T, int L>
-size_t row_smem() { return row_base_smem<T, L>() + row_pf_bytes<T, L>(row_depth<T, L>()); }
+template <typename T, int L, int NFX = row_nfx<T, L>()>
+size_t row_smem() { return row_base_smem<T, L, NFX>() + row_pf_bytes<T, L>(row_depth<T, L, NFX>()); }
 // The stage pass without inverse transforms (the last stage of a step): one
-// exchange buffer per row pair, registers as row_min_blocks<.., 1>; prefetch
+// exchange buffer per row pair, registers as row_min_blocks<.., 0>; prefetch
 // depth again occupancy first.
 template <typename T, int L>
 constexpr size_t rowx_smem(int depth) {
-  return (size_t)rows_per_cta<T, L>() * spad_size<row_radix<T, L>()>(1 << L) * sizeof(typename Cplx<T>::type) +
-         row_pf_bytes<T, L>(depth);
+  return (size_t)rowx_rpc<T, L>() * (spad_size<rowx_radix<T, L>()>(1 << L) + depth * 4 * rowx_group<T, L>()) *
+         sizeof(typename Cplx<T>::type);
 }
 template <typename T, int L>
 constexpr int rowx_occupancy(int depth) {
-  constexpr int by_regs = row_min_blocks<T, row_radix<T, L>(), 1>(rows_per_cta<T, L>() * row_group<T, L>());
+  constexpr int by_regs = row_min_blocks<T, rowx_radix<T, L>(), 0>(rowx_rpc<T, L>() * rowx_group<T, L>());
   const size_t smem = rowx_smem<T, L>(depth);
   if (smem > 220 * 1024) return 0;
   const int by_smem = (int)((227 * 1024) / (smem + 1024));
@@ -113,7 +130,7 @@ constexpr int rowx_occupancy(int depth) {
 }
 template <typename T, int L>
 constexpr int rowx_depth() {
-  constexpr int R = row_radix<T, L>();
+  constexpr int R = rowx_radix<T, L>();
   int best = 1, occ = rowx_occupancy<T, L>(1);
   for (int d = 2; d <= R; d *= 2) {
     const int o = rowx_occupancy<T, L>(d);
@@ -149,9 +166,20 @@ cudaError_t launch_row_t(const KP& kp, const RowArgs& a, cudaStream_t st) {
   constexpr int N = 1 << L, RPC = rows_per_cta<T, L>();
   const int rpc = a.rpc > 0 ? a.rpc : RPC;
   const int grid = (N / 2 + 1 + rpc - 1) / rpc;
-  if (a.rmode == RM_STAGE && !a.do_p1)
-    return launch_pdl(k_row<T, L, row_radix<T, L>(), RPC, rowx_depth<T, L>(), 1>, dim3(grid),
-                      dim3(rpc * row_group<T, L>()), rowx_smem<T, L>(rowx_depth<T, L>()) / RPC * rpc, st, kp, a);
+  if (a.rmode == RM_STAGE && !a.do_p1) {  // last stage: its own radix, the compiled launch shape
+    constexpr int RPCX = rowx_rpc<T, L>();
+    RowArgs ax = a;
+    ax.rpc = 0;
+    return launch_pdl(k_row<T, L, rowx_radix<T, L>(), RPCX, rowx_depth<T, L>(), 0>,
+                      dim3((N / 2 + 1 + RPCX - 1) / RPCX), dim3(RPCX * rowx_group<T, L>()),
+                      rowx_smem<T, L>(rowx_depth<T, L>()), st, kp, ax);
+  }
+  if constexpr (row_nfx_scalar<T, L>() != row_nfx<T, L>()) {
+    constexpr int NS = row_nfx_scalar<T, L>();
+    if (a.fmode == FM_SCAL && a.rmode == RM_STAGE)
+      return launch_pdl(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L, NS>(), NS>, dim3(grid),
+                        dim3(rpc * row_group<T, L>()), row_smem<T, L, NS>() / RPC * rpc, st, kp, a);
+  }
   return launch_pdl(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>, dim3(grid),
                     dim3(rpc * row_group<T, L>()), row_smem<T, L>() / RPC * rpc, st, kp, a);
 }
@@ -175,7 +203,13 @@ cudaError_t set_attrs_t() {
   cudaError_t e = cudaFuncSetAttribute(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem<T, L>());
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_row<T, L, row_radix<T, L>(), RPC, rowx_depth<T, L>(), 1>,
+  if constexpr (row_nfx_scalar<T, L>() != row_nfx<T, L>()) {
+    constexpr int NS = row_nfx_scalar<T, L>();
+    e = cudaFuncSetAttribute(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L, NS>(), NS>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem<T, L, NS>());
+    if (e != cudaSuccess) return e;
+  }
+  e = cudaFuncSetAttribute(k_row<T, L, rowx_radix<T, L>(), rowx_rpc<T, L>(), rowx_depth<T, L>(), 0>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rowx_smem<T, L>(rowx_depth<T, L>()));
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>()>,
