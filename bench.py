@@ -561,8 +561,9 @@ def main():
                 "members": len(members), "passive_scalars": n_scal, "steps": steps, "finite": finite,
                 "gpu_launches_per_step": ens.launches_per_step(),
                 "config": "48x128^2 + 32x256^2 + 16x512^2, alpha in {0,.5,1,1.5}, 0-3 scalars, FP32 IF-RK4, "
-                          "nu=1e-6 p=8 dt=5e-4, one CUDA graph per size class per step, no L2 flush "
-                          "(working set > L2)"}
+                          "nu=1e-6 p=8 dt=5e-4, one launch per pass of every RK stage over all sizes and "
+                          "scalars (scalars one step behind theta), the step replayed from one CUDA graph, "
+                          "no L2 flush (working set > L2)"}
 
     def measure_closure(steps=300, warmup=20):
         """Closure-vs-DNS GPU time per unit of simulated time: the coarse

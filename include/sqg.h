@@ -261,6 +261,23 @@ int sqg_batch_multistep(sqg_batch* batch, int32_t n_steps, double dt, int32_t us
 int sqg_batch_last_launch_count(const sqg_batch* batch, int64_t* launches);
 int sqg_batch_destroy(sqg_batch* batch);
 
+/* Multi-size ensembles (the pmap ensemble of multi_gpu.py:118-155, for
+ * members of uneven resolution): the members of up to three batches of
+ * distinct size classes N = 128, 256, 512 (same precision and scheme) advance
+ * in ONE launch per pass of every RK stage -- eight launches per step for
+ * theta and every scalar of every member.  The scalars run one step behind
+ * theta inside the same launches (the scalar step that needs u, v of
+ * theta_{n+1} runs beside theta's step n+2 and transforms u, v from the half
+ * spectra that step reads), so sqg_ensemble_multistep(n) gives the same
+ * states as n batch steps: theta first, then the scalars with theta's new
+ * velocity (solver_with_scalars.py:131-178).  The batches keep owning the
+ * member buffers; destroy the ensemble before them. */
+typedef struct sqg_ensemble sqg_ensemble;
+int sqg_ensemble_create(sqg_batch* const* classes, int32_t n_classes, sqg_ensemble** out);
+int sqg_ensemble_multistep(sqg_ensemble* ensemble, int32_t n_steps, double dt, int32_t use_graph, void* stream);
+int sqg_ensemble_last_launch_count(const sqg_ensemble* ensemble, int64_t* launches);
+int sqg_ensemble_destroy(sqg_ensemble* ensemble);
+
 /* Reads and clears the sticky status flags (bit 0: non-finite value seen).
  * Synchronises the stream. */
 int sqg_check_status(sqg_plan* plan, uint32_t* flags, void* stream);

@@ -109,6 +109,10 @@ SIGNATURES = {
     "sqg_batch_multistep": [_vp, _i32, _dbl, _i32, _vp],
     "sqg_batch_last_launch_count": [_vp, C.POINTER(C.c_int64)],
     "sqg_batch_destroy": [_vp],
+    "sqg_ensemble_create": [C.POINTER(C.c_void_p), _i32, C.POINTER(C.c_void_p)],
+    "sqg_ensemble_multistep": [_vp, _i32, _dbl, _i32, _vp],
+    "sqg_ensemble_last_launch_count": [_vp, C.POINTER(C.c_int64)],
+    "sqg_ensemble_destroy": [_vp],
     "closure_conv64": [_i32, _i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp],
     "closure_wgrad64": [_i32, _i32, _i32, _vp, _vp, _vp, _i32, _vp, _vp, _vp],
     "closure_conv_in": [_i32, _i32, _i32, C.c_float, _vp, _vp, _vp, _vp, _vp, _vp],

@@ -1348,6 +1348,8 @@ struct sqg_batch {
   RowArgs* d_sp1 = nullptr;      // [S]
   ColArgs* d_scol = nullptr;     // [S]
   RowArgs* d_srow = nullptr;     // [4][S]
+  ColArgs* d_scolv = nullptr;    // [S] first scalar stage with u, v from theta's spectra (multi-size path)
+  RowArgs* d_srow4p = nullptr;   // [S] last scalar stage that also transforms s_{n+1} (multi-size path)
   double args_dt = -1.0;
   bool ready = false;
   cudaGraphExec_t graph = nullptr;
@@ -1393,7 +1395,8 @@ int batch_upload_args(sqg_batch* b, double dt, cudaStream_t st) {
   base.n_ring = 0;
   std::vector<KP> kp(M), kps(std::max(S, 1));
   std::vector<RowArgs> p1(M), row(4 * M), sp1(std::max(S, 1)), srow(4 * std::max(S, 1));
-  std::vector<ColArgs> col(M), vel(M), scol(std::max(S, 1));
+  std::vector<ColArgs> col(M), vel(M), scol(std::max(S, 1)), scolv(std::max(S, 1));
+  std::vector<RowArgs> srow4p(std::max(S, 1));
   const bool explicit_lin = b->d.scheme == SQG_EXPLICIT_RK4 &&
                             (b->d.nu_p != 0.0 || (b->d.has_damping && (b->d.mu != 0.0 || b->d.nu_damp != 0.0)));
   for (int i = 0; i < M; ++i) {
@@ -1469,6 +1472,17 @@ int batch_upload_args(sqg_batch* b, double dt, cudaStream_t st) {
     c.jh = const_cast<void*>(a.jh);
     c.uv = mb + b->m_uv;
     scol[k] = c;
+    // multi-size path: stage 1 transforms theta's u, v itself (its first
+    // scalar writes u + i v for stages 2-4), and stage 4 also transforms
+    // s_{n+1} for the next step
+    ColArgs cv = c;
+    cv.cmode = CM_SCALV;
+    cv.xh = mb + b->m_xh;
+    cv.xh2 = a.xh;
+    cv.out0 = q == 0 ? mb + b->m_uv : nullptr;
+    scolv[k] = cv;
+    srow4p[k] = srow[3 * std::max(S, 1) + k];
+    srow4p[k].do_p1 = 1;
   }
   auto up = [&](void* dst, const void* src, size_t n) {
     return cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, st);
@@ -1483,6 +1497,8 @@ int batch_upload_args(sqg_batch* b, double dt, cudaStream_t st) {
     SQG_CUDA(up(b->d_sp1, sp1.data(), S * sizeof(RowArgs)));
     SQG_CUDA(up(b->d_srow, srow.data(), 4 * S * sizeof(RowArgs)));
     SQG_CUDA(up(b->d_scol, scol.data(), S * sizeof(ColArgs)));
+    SQG_CUDA(up(b->d_scolv, scolv.data(), S * sizeof(ColArgs)));
+    SQG_CUDA(up(b->d_srow4p, srow4p.data(), S * sizeof(RowArgs)));
   }
   SQG_CUDA(cudaStreamSynchronize(st));  // host vectors go out of scope
   b->args_dt = dt;
@@ -1563,7 +1579,8 @@ int sqg_batch_create(const sqg_desc* desc, int32_t n_members, const sqg_member* 
   const size_t Sx = std::max(b->S, 1);
   b->off_total = b->off_args + al(b->M * sizeof(KP)) + al(Sx * sizeof(KP)) + al(b->M * sizeof(RowArgs)) +
                  al(b->M * sizeof(ColArgs)) + al(4 * b->M * sizeof(RowArgs)) + al(b->M * sizeof(ColArgs)) +
-                 al(Sx * sizeof(RowArgs)) + al(Sx * sizeof(ColArgs)) + al(4 * Sx * sizeof(RowArgs));
+                 al(Sx * sizeof(RowArgs)) + al(Sx * sizeof(ColArgs)) + al(4 * Sx * sizeof(RowArgs)) +
+                 al(Sx * sizeof(ColArgs)) + al(Sx * sizeof(RowArgs));
   *out = b;
   return SQG_OK;
 }
@@ -1594,6 +1611,8 @@ int sqg_batch_set_workspace(sqg_batch* b, void* ws, size_t bytes, void* stream) 
   b->d_sp1 = (RowArgs*)take(Sx * sizeof(RowArgs));
   b->d_scol = (ColArgs*)take(Sx * sizeof(ColArgs));
   b->d_srow = (RowArgs*)take(4 * Sx * sizeof(RowArgs));
+  b->d_scolv = (ColArgs*)take(Sx * sizeof(ColArgs));
+  b->d_srow4p = (RowArgs*)take(Sx * sizeof(RowArgs));
   if (b->d.precision == SQG_F64) { SQG_CUDA(set_batch_attrs_p<double>(b->log2N)); }
   else { SQG_CUDA(set_batch_attrs_p<float>(b->log2N)); }
   if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
@@ -1668,6 +1687,201 @@ int sqg_batch_destroy(sqg_batch* b) {
   b->tables.cap_stream = nullptr;
   b->tables.ev_in = b->tables.ev_out = nullptr;
   delete b;
+  return SQG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Multi-size ensembles: the members of several batches (size classes
+// N = 128, 256, 512) advance in one launch per pass of every RK stage.  The
+// scalars run one step behind theta in the same launches: the scalar step
+// that needs u, v of theta_{n+1} (frozen over its stages) runs beside theta's
+// step n+2, whose first column pass reads the half spectra of theta_{n+1};
+// the scalar's first column pass transforms u and v from them.  multistep(n)
+// is: the input transforms of theta_0 and s_0 (one launch), theta's first
+// step alone, n - 1 fused steps (replayed from one CUDA graph) and the last
+// scalar step alone -- the same arithmetic as stepping theta and then the
+// scalars, step after step.
+// ---------------------------------------------------------------------------
+struct sqg_ensemble {
+  std::vector<sqg_batch*> cls;
+  int precision = SQG_F32;
+  cudaGraphExec_t graph = nullptr;
+  double graph_dt = -1.0;
+  cudaStream_t cap = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  int64_t launches = 0;
+};
+
+namespace {
+
+enum { EK_P1 = 0, EK_COL = 1, EK_ROW = 2 };
+
+// Segments of one multi-size launch: kind EK_*, RK stage s (1..4), which
+// entities take part, and whether the scalars run pipelined (their first
+// stage transforms u, v; their last stage also transforms s_{n+1}).
+int ens_segments(const sqg_ensemble* e, int kind, int s, bool theta, bool scalars, MultiArgs& ma) {
+  std::memset(&ma, 0, sizeof(ma));
+  int blocks = 0;
+  auto add = [&](int log2n, int tiles, int count, const KP* kps, const void* args) {
+    if (count <= 0) return;
+    MultiSeg& g = ma.seg[ma.nseg++];
+    g.start = blocks;
+    g.tiles = tiles;
+    g.log2n = log2n;
+    g.kps = kps;
+    g.args = args;
+    blocks += tiles * count;
+  };
+  const bool f64 = e->precision == SQG_F64;
+  for (int pass = 0; pass < 2; ++pass) {  // theta segments first, then the scalars
+    for (sqg_batch* b : e->cls) {
+      const int L = b->log2N;
+      const int tiles = kind == EK_COL ? (f64 ? multi_col_tiles<double>(L) : multi_col_tiles<float>(L))
+                                       : (f64 ? multi_row_tiles<double>(L) : multi_row_tiles<float>(L));
+      if (pass == 0 && theta) {
+        const void* args = kind == EK_P1 ? (const void*)b->d_p1
+                           : kind == EK_COL ? (const void*)b->d_col : (const void*)(b->d_row + (size_t)(s - 1) * b->M);
+        add(L, tiles, b->M, b->d_kp, args);
+      }
+      if (pass == 1 && scalars && b->S > 0) {
+        const void* args;
+        if (kind == EK_P1) args = b->d_sp1;
+        else if (kind == EK_COL) args = s == 1 ? (const void*)b->d_scolv : (const void*)b->d_scol;
+        else args = (s == 4 && theta) ? (const void*)b->d_srow4p : (const void*)(b->d_srow + (size_t)(s - 1) * b->S);
+        add(L, tiles, b->S, b->d_kps, args);
+      }
+    }
+  }
+  return blocks;
+}
+
+cudaError_t ens_launch(sqg_ensemble* e, int kind, int s, bool theta, bool scalars, cudaStream_t st) {
+  MultiArgs ma;
+  const int blocks = ens_segments(e, kind, s, theta, scalars, ma);
+  if (blocks == 0) return cudaSuccess;
+  e->launches++;
+  const bool f64 = e->precision == SQG_F64;
+  if (kind == EK_COL) return f64 ? launch_col_multi<double>(ma, blocks, st) : launch_col_multi<float>(ma, blocks, st);
+  return f64 ? launch_row_multi<double>(ma, blocks, st) : launch_row_multi<float>(ma, blocks, st);
+}
+
+// One RK step: the four stages of the given entities.
+cudaError_t ens_step(sqg_ensemble* e, bool theta, bool scalars, cudaStream_t st) {
+  for (int s = 1; s <= 4; ++s) {
+    cudaError_t c = ens_launch(e, EK_COL, s, theta, scalars, st);
+    if (c != cudaSuccess) return c;
+    if ((c = ens_launch(e, EK_ROW, s, theta, scalars, st)) != cudaSuccess) return c;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sqg_ensemble_create(sqg_batch* const* classes, int32_t n_classes, sqg_ensemble** out) {
+  if (!classes || !out || n_classes < 1 || n_classes > 3) return fail(SQG_ERR_INVALID, "1 to 3 size classes");
+  sqg_ensemble* e = new sqg_ensemble();
+  for (int i = 0; i < n_classes; ++i) {
+    sqg_batch* b = classes[i];
+    std::string why;
+    if (!b) why = "null batch";
+    else if (!b->ready) why = "batch workspace not set";
+    else if (b->log2N < kMultiLo || b->log2N > kMultiHi) why = "multi-size launches serve N = 128, 256, 512";
+    else if (i > 0 && b->d.precision != classes[0]->d.precision) why = "all classes need the same precision";
+    else if (i > 0 && b->d.scheme != classes[0]->d.scheme) why = "all classes need the same time scheme";
+    for (int k = 0; k < i && why.empty(); ++k)
+      if (classes[k]->log2N == b->log2N) why = "each size class at most once";
+    if (!why.empty()) { delete e; return fail(SQG_ERR_INVALID, "sqg_ensemble_create: " + why); }
+    e->cls.push_back(b);
+  }
+  e->precision = classes[0]->d.precision;
+  cudaError_t c = e->precision == SQG_F64 ? set_multi_attrs<double>() : set_multi_attrs<float>();
+  if (c != cudaSuccess) { delete e; return fail(SQG_ERR_CUDA, std::string("multi-size kernels: ") + cudaGetErrorString(c)); }
+  *out = e;
+  return SQG_OK;
+}
+
+int sqg_ensemble_multistep(sqg_ensemble* e, int32_t n_steps, double dt, int32_t use_graph, void* stream) {
+  if (!e) return fail(SQG_ERR_INVALID, "null ensemble");
+  if (n_steps < 0) return fail(SQG_ERR_INVALID, "n_steps must be >= 0");
+  if (n_steps == 0) return SQG_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  bool any_scalars = false;
+  for (sqg_batch* b : e->cls) {
+    if (b->args_dt != dt) {
+      if ((rc = batch_upload_args(b, dt, st)) != SQG_OK) return rc;
+      if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+    }
+    any_scalars |= b->S > 0;
+  }
+  if (e->graph && e->graph_dt != dt) { cudaGraphExecDestroy(e->graph); e->graph = nullptr; }
+  e->launches = 0;
+  // input transforms of theta_0 and s_0, then theta's first step alone
+  SQG_CUDA(ens_launch(e, EK_P1, 1, true, true, st));
+  SQG_CUDA(ens_step(e, true, false, st));
+  if (n_steps > 1) {
+    if (!use_graph) {
+      for (int n = 1; n < n_steps; ++n) SQG_CUDA(ens_step(e, true, true, st));
+    } else {
+      if (!e->cap) {
+        SQG_CUDA(cudaStreamCreateWithFlags(&e->cap, cudaStreamNonBlocking));
+        SQG_CUDA(cudaEventCreateWithFlags(&e->ev_in, cudaEventDisableTiming));
+        SQG_CUDA(cudaEventCreateWithFlags(&e->ev_out, cudaEventDisableTiming));
+      }
+      int64_t per = 0;
+      if (!e->graph) {
+        cudaGraph_t g;
+        SQG_CUDA(cudaStreamBeginCapture(e->cap, cudaStreamCaptureModeThreadLocal));
+        const int64_t saved = e->launches;
+        cudaError_t c = ens_step(e, true, true, e->cap);
+        cudaError_t ce = cudaStreamEndCapture(e->cap, &g);
+        per = e->launches - saved;
+        e->launches = saved;
+        if (c != cudaSuccess) return fail(SQG_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(c));
+        if (ce != cudaSuccess) return fail(SQG_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&e->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return fail(SQG_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(ce));
+        e->graph_dt = dt;
+      } else {
+        MultiArgs ma;
+        for (int s = 1; s <= 4; ++s) {
+          per += ens_segments(e, EK_COL, s, true, true, ma) > 0;
+          per += ens_segments(e, EK_ROW, s, true, true, ma) > 0;
+        }
+      }
+      SQG_CUDA(cudaEventRecord(e->ev_in, st));
+      SQG_CUDA(cudaStreamWaitEvent(e->cap, e->ev_in, 0));
+      for (int n = 1; n < n_steps; ++n) {
+        SQG_CUDA(cudaGraphLaunch(e->graph, e->cap));
+        e->launches += per;
+      }
+      SQG_CUDA(cudaEventRecord(e->ev_out, e->cap));
+      SQG_CUDA(cudaStreamWaitEvent(st, e->ev_out, 0));
+    }
+  }
+  // the scalars' last step (with u, v of the final theta)
+  if (any_scalars) SQG_CUDA(ens_step(e, false, true, st));
+  return SQG_OK;
+}
+
+int sqg_ensemble_last_launch_count(const sqg_ensemble* e, int64_t* n) {
+  if (!e || !n) return fail(SQG_ERR_INVALID, "null argument");
+  *n = e->launches;
+  return SQG_OK;
+}
+
+int sqg_ensemble_destroy(sqg_ensemble* e) {
+  if (!e) return SQG_OK;
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  if (e->cap) cudaStreamDestroy(e->cap);
+  if (e->ev_in) cudaEventDestroy(e->ev_in);
+  if (e->ev_out) cudaEventDestroy(e->ev_out);
+  delete e;
   return SQG_OK;
 }
 

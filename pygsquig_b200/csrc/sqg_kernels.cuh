@@ -301,7 +301,7 @@ __device__ __forceinline__ void row_sources(const KP& kp, const RowArgs& a, HA h
 // cp.async ahead of use; the first DEPTH chunks are requested before the
 // forward FFT of the J row, so their latency hides behind it.
 template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
-__device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a) {
+__device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int tile) {
   using C = typename Cplx<T>::type;
   constexpr int N = 1 << LOG2N;
   constexpr int G = N / R;
@@ -317,7 +317,7 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a) {
   const int rpc = a.rpc > 0 ? a.rpc : RPC;  // launch shape (autotuned), <= RPC
   C* pf = smem + (size_t)rpc * NB * XB + (size_t)grp * (DEPTH * 4 * G);
   static_assert(NFX != 1 || DEPTH * 4 * G >= 2 * N, "the one-field pass keeps h and an in the staging slots");
-  const int p_raw = blockIdx.x * rpc + grp;
+  const int p_raw = tile * rpc + grp;
   const bool valid = p_raw <= H;
   const int p = valid ? p_raw : H;
   const int pp = (N - p) & (N - 1);
@@ -615,11 +615,16 @@ struct RingCtl {
   int pad;
 };
 
-enum ColMode { CM_THETA = 0, CM_SCAL = 1, CM_VEL = 2, CM_PHYS1 = 3, CM_FWD = 4 };
+// CM_SCALV: the first scalar stage of an ensemble step, with u and v
+// transformed from theta's half spectra (xh fields 0, 1) beside the scalar's
+// s_x, s_y (xh2 fields 0, 1); writes u + i v for the later stages (out0, if
+// set).  Needs all four field buffers (NBUF = 4).
+enum ColMode { CM_THETA = 0, CM_SCAL = 1, CM_VEL = 2, CM_PHYS1 = 3, CM_FWD = 4, CM_SCALV = 5 };
 
 struct ColArgs {
   int cmode;
   const void* xh;   // nf x (N/2+1) x N
+  const void* xh2;  // CM_SCALV: the scalar's s_x, s_y half spectra
   void* jh;         // (N/2+1) x N
   const void* uv;   // N x N complex u + i v (CM_SCAL input)
   void* out0;       // CM_VEL: u (real N x N) or uv complex; CM_PHYS1: real field
@@ -724,7 +729,7 @@ __device__ void ring_reduce(const KP& kp, const ColArgs& a);
 // once (round-2 copies land while round 1 computes); NBUF = 2: two rounds of
 // two fields (large N in float64, where four buffers do not fit).
 template <typename T, int LOG2N, int R, int NP, int NBUF>
-__device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
+__device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int tile, int ntiles) {
   using C = typename Cplx<T>::type;
   constexpr int N = 1 << LOG2N;
   constexpr int G = N / R;
@@ -732,7 +737,7 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
   constexpr int SZ = ColBuf<N, R>::SZ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* smem = reinterpret_cast<C*>(smem_raw);
-  if (a.ring_cta && blockIdx.x == gridDim.x - 1) {
+  if (a.ring_cta && tile == ntiles - 1) {
     ring_reduce<T, LOG2N>(kp, a);
     return;
   }
@@ -741,7 +746,7 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
   const int np = a.np > 0 ? a.np : NP;       // launch shape (autotuned), <= NP
   constexpr int qs = NBUF * SZ;              // slots per column pair
   C* gbuf = smem + (size_t)grp * qs;         // this group's NBUF buffers
-  const int y0 = blockIdx.x * (2 * np);
+  const int y0 = tile * (2 * np);
   const int ya = y0 + 2 * grp;
   const C* __restrict__ tw = reinterpret_cast<const C*>(kp.tw);
   const C* xh = reinterpret_cast<const C*>(a.xh);
@@ -808,14 +813,18 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
   C W[R];
 #pragma unroll
   for (int m = 0; m < R; ++m) W[m] = mkc<C>(0, 0);
-  const int nround = a.cmode == CM_THETA ? 2 : (a.cmode == CM_SCAL ? 1 : 0);
+  if (NBUF != 4 && a.cmode == CM_SCALV) return;  // not supported (the host never asks for it)
+  const int nround = (a.cmode == CM_THETA || a.cmode == CM_SCALV) ? 2 : (a.cmode == CM_SCAL ? 1 : 0);
   const int fa0 = 0, fb0 = a.cmode == CM_THETA ? 2 : 1, fa1 = 1, fb1 = 3;
   if (nround > 0) {
+    // CM_SCALV: buffers (u, s_x, v, s_y) -- u, v from theta's xh, s_x, s_y from xh2
+    const C* xb = a.cmode == CM_SCALV ? reinterpret_cast<const C*>(a.xh2) : xh;
+    const int fb0s = a.cmode == CM_SCALV ? 0 : fb0, fb1s = a.cmode == CM_SCALV ? 1 : fb1;
     col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa0 * fstride, y0, 0, smem, np);
-    col_fetch<T, LOG2N, R, NP, NBUF>(xh + fb0 * fstride, y0, 1, smem, np);
+    col_fetch<T, LOG2N, R, NP, NBUF>(xb + fb0s * fstride, y0, 1, smem, np);
     if (NBUF == 4 && nround == 2) {
       col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa1 * fstride, y0, 2, smem, np);
-      col_fetch<T, LOG2N, R, NP, NBUF>(xh + fb1 * fstride, y0, 3, smem, np);
+      col_fetch<T, LOG2N, R, NP, NBUF>(xb + fb1s * fstride, y0, 3, smem, np);
     }
     cp_async_commit();
   }
@@ -835,10 +844,17 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a) {
     for (int f = 0; f < 4; ++f) col_first_load<T, LOG2N, R>(gbuf + f * SZ, j, V[f]);
     fft_multi<T, LOG2N, R, +1, 4>(V, gbuf, SZ, j, tw);
     // J = u theta_x + v theta_y for columns a (real parts) and b (imaginary)
+    // (CM_SCALV: u s_x + v s_y)
 #pragma unroll
     for (int m = 0; m < R; ++m) {
       W[m].x = V[0][m].x * V[1][m].x + V[2][m].x * V[3][m].x;
       W[m].y = V[0][m].y * V[1][m].y + V[2][m].y * V[3][m].y;
+    }
+    if (a.cmode == CM_SCALV && a.out0) {  // u + i v for the later stages (column-pair-major)
+      C* o = reinterpret_cast<C*>(a.out0);
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+        store_pair(o + uv_index(N, j + m * G, ya), mkc<C>(V[0][m].x, V[2][m].x), mkc<C>(V[0][m].y, V[2][m].y));
     }
     if (a.in_real) {  // physical-space source: J - src
       const T* f = reinterpret_cast<const T*>(a.in_real);
@@ -1005,14 +1021,14 @@ template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
 __global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), row_min_blocks<T, R, NFX>(RPC * ((1 << LOG2N) / R)))
 k_row(KP kp, RowArgs a) {
   pdl_wait();
-  row_body<T, LOG2N, R, RPC, DEPTH, NFX>(kp, a);
+  row_body<T, LOG2N, R, RPC, DEPTH, NFX>(kp, a, blockIdx.x);
 }
 
 template <typename T, int LOG2N, int R, int NP, int NBUF>
 __global__ void __launch_bounds__(NP * ((1 << LOG2N) / R), min_blocks_r<T, R>(NP * ((1 << LOG2N) / R)))
 k_col(KP kp, ColArgs a) {
   pdl_wait();
-  col_body<T, LOG2N, R, NP, NBUF>(kp, a);
+  col_body<T, LOG2N, R, NP, NBUF>(kp, a, blockIdx.x, gridDim.x);
 }
 
 // Batched forms: the member's parameters come from device arrays; members
@@ -1021,19 +1037,19 @@ template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
 __global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), row_min_blocks<T, R, NFX>(RPC * ((1 << LOG2N) / R)))
 k_row_batch(const KP* __restrict__ kps, const RowArgs* __restrict__ as) {
   pdl_wait();
-  const KP kp = kps[blockIdx.y];
-  const RowArgs a = as[blockIdx.y];
+  const KP& kp = kps[blockIdx.y];  // read in place (a local copy would be indexed dynamically)
+  const RowArgs& a = as[blockIdx.y];
   if (a.xh == nullptr && a.rhs_out == nullptr) return;
-  row_body<T, LOG2N, R, RPC, DEPTH, NFX>(kp, a);
+  row_body<T, LOG2N, R, RPC, DEPTH, NFX>(kp, a, blockIdx.x);
 }
 
 template <typename T, int LOG2N, int R, int NP, int NBUF>
 __global__ void __launch_bounds__(NP * ((1 << LOG2N) / R), min_blocks_r<T, R>(NP * ((1 << LOG2N) / R)))
 k_col_batch(const KP* __restrict__ kps, const ColArgs* __restrict__ as) {
   pdl_wait();
-  const KP kp = kps[blockIdx.y];
-  const ColArgs a = as[blockIdx.y];
+  const KP& kp = kps[blockIdx.y];
+  const ColArgs& a = as[blockIdx.y];
   if (a.xh == nullptr) return;
-  col_body<T, LOG2N, R, NP, NBUF>(kp, a);
+  col_body<T, LOG2N, R, NP, NBUF>(kp, a, blockIdx.x, gridDim.x);
 }
 }  // namespace sqg

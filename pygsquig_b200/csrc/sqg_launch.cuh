@@ -153,6 +153,37 @@ template <typename T, int L> cudaError_t launch_row_batch_t(const KP* kps, const
 template <typename T, int L> cudaError_t launch_col_batch_t(const KP* kps, const ColArgs* as, int members, cudaStream_t st);
 template <typename T, int L> cudaError_t set_batch_attrs_t();
 
+// ---- multi-size ensemble passes ----
+// One launch covers every entity (theta of a member, or one passive scalar)
+// of several size classes.  The blocks are laid out by segment: segment g
+// holds the entities of one class and one kind, tiles blocks per entity from
+// block seg[g].start on; a block finds its segment, entity and tile and runs
+// the single-field pass body of its class.  The classes N = 128, 256, 512
+// share the block shapes (128-thread row blocks, 256-thread column blocks),
+// so one launch configuration serves them all.
+struct MultiSeg {
+  int start;         // first block of the segment
+  int tiles;         // blocks per entity
+  int log2n;         // size class
+  int pad;
+  const KP* kps;     // per entity
+  const void* args;  // RowArgs[] or ColArgs[] per entity
+};
+constexpr int kMultiSegs = 8;
+struct MultiArgs {
+  int nseg;
+  int pad;
+  MultiSeg seg[kMultiSegs];
+};
+constexpr int kMultiLo = 7, kMultiHi = 9;  // log2 N of the classes a multi-size launch serves
+constexpr int kMultiRowThreads = 128, kMultiColThreads = 256;
+template <typename T> cudaError_t launch_row_multi(const MultiArgs& ma, int blocks, cudaStream_t st);
+template <typename T> cudaError_t launch_col_multi(const MultiArgs& ma, int blocks, cudaStream_t st);
+template <typename T> cudaError_t set_multi_attrs();
+// row pairs (column pairs) per block of class log2n in a multi-size launch
+template <typename T> int multi_row_tiles(int log2n);
+template <typename T> int multi_col_tiles(int log2n);
+
 #ifdef SQG_LAUNCH_DEFS
 // Launch shapes: a.rpc row pairs per CTA of the row pass (a.np column pairs
 // per CTA of the column pass), a power-of-two divisor of the compiled maximum;

@@ -7,6 +7,12 @@ members of the class (alpha and the passive scalars vary per member), and a
 whole step of the class is replayed from one CUDA graph.  Members of
 different N form separate classes.
 
+When every size class is one of N = 128, 256, 512 (the default ``unified``
+mode), the classes advance together: one launch per pass of every RK stage
+covers every member and every scalar of every class (eight launches per
+step), with the scalars one step behind theta inside the same launches
+(``sqg_ensemble_multistep``).  Other sizes step class by class.
+
 Each member is a gSQG field with its own alpha and 0..4 passive scalars
 (diffusivity kappa, no source), stepped like
 ``gSQGSolverWithScalars.step``: theta first, then the scalars with theta's
@@ -84,11 +90,42 @@ class _Batch:
             pass
 
 
+UNIFIED_SIZES = (128, 256, 512)
+
+
+class _Unified:
+    """The size classes' batches advanced by one multi-size launch per pass."""
+
+    def __init__(self, batches):
+        lib = _lib.load()
+        arr = (C.c_void_p * len(batches))(*[b._h.value for b in batches])
+        h = C.c_void_p()
+        _lib.check(lib.sqg_ensemble_create(arr, len(batches), C.byref(h)))
+        self._h, self._lib, self._batches = h, lib, batches  # the batches outlive the ensemble
+
+    def multistep(self, n, dt, use_graph=True):
+        _lib.check(self._lib.sqg_ensemble_multistep(self._h, int(n), float(dt), 1 if use_graph else 0,
+                                                    _stream_ptr()))
+
+    def launches(self):
+        n = C.c_int64()
+        _lib.check(self._lib.sqg_ensemble_last_launch_count(self._h, C.byref(n)))
+        return int(n.value)
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                self._lib.sqg_ensemble_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
 class EnsembleSolver:
     """Advances a list of members together (all states stay on the GPU)."""
 
     def __init__(self, members: Sequence[Member], nu_p: float = 0.0, p: int = 8, L: float = TWO_PI,
-                 precision: str = "float32", scheme: str = "ifrk4"):
+                 precision: str = "float32", scheme: str = "ifrk4", unified: bool = True):
         if p not in (2, 4, 8):
             raise ValueError(f"p must be 2, 4, or 8, got {p}")
         self.members = list(members)
@@ -108,22 +145,31 @@ class EnsembleSolver:
             b = _Batch(N, L, [self.members[i] for i in idx], nu_p, p, precision, scheme,
                        [self.theta[i] for i in idx], [self.scalars[i] for i in idx])
             self.classes[N] = (idx, b)
+        self.unified = None
+        if unified and set(self.classes) <= set(UNIFIED_SIZES):
+            self.unified = _Unified([b for _, (_, b) in sorted(self.classes.items())])
         self.time = 0.0
         self.step_count = 0
 
     def multistep(self, n_steps: int, dt: float, use_graph: bool = True) -> None:
-        for _, (_, b) in self.classes.items():
-            b.multistep(n_steps, dt, use_graph)
+        if self.unified is not None:
+            self.unified.multistep(n_steps, dt, use_graph)
+        else:
+            for _, (_, b) in self.classes.items():
+                b.multistep(n_steps, dt, use_graph)
         self.time += n_steps * dt
         self.step_count += n_steps
         self._last_n = n_steps
 
     def launches_per_step(self) -> float:
-        """Kernel launches per ensemble step in the last multistep call (the
-        one input pass per size class at the start excluded)."""
+        """Kernel launches per ensemble step in the last multistep call
+        (class by class: the one input pass per size class at the start
+        excluded; unified: every launch of the call, divided by its steps)."""
         n = getattr(self, "_last_n", 0)
         if not n:
             return 0.0
+        if self.unified is not None:
+            return self.unified.launches() / n
         return (sum(b.launches() for _, (_, b) in self.classes.items()) - len(self.classes)) / n
 
     def state(self, i: int) -> dict:
