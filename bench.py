@@ -337,6 +337,8 @@ def main():
     ap.add_argument("--precision", default="float32", choices=["float32", "float64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="auto", help="extra measured variants: auto|none")
+    ap.add_argument("--profile-range", action="store_true",
+                    help="bracket the first timed step with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     args = ap.parse_args()
     w = WORKLOADS.get(args.workload, WORKLOADS["hires4096"])
     if args.impl == "reference":
@@ -410,7 +412,7 @@ def main():
                                          diagnostics={})
         return c
 
-    def measure(workload, prec, steps, warmup, with_e2e, with_clocks):
+    def measure(workload, prec, steps, warmup, with_e2e, with_clocks, profile_range=False):
         w, g, s, st, one, noise_host, n_ring, ring, damp = setup(workload, prec, warmup + steps + 1)
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
         stream = torch.cuda.current_stream()
@@ -427,9 +429,13 @@ def main():
         t_wall0 = time.time()
         launches = 0
         for k in range(steps):
+            if profile_range and k == 0:
+                torch.cuda.cudart().cudaProfilerStart()
             evs[k][0].record(stream)
             st = one(warmup + k, st)
             evs[k][1].record(stream)
+            if profile_range and k == 0:
+                torch.cuda.cudart().cudaProfilerStop()
             launches += pl.last_launch_count()
             flush.zero_()
         torch.cuda.synchronize()
@@ -556,7 +562,14 @@ def main():
         ms = replicas.max_over_ranks(ms, "cuda")
         finite = all(bool(torch.isfinite(torch.view_as_real(t)).all().item()) for t in ens.theta)
         n_scal = sum(len(m.scalars0) for m in members)
+        # the step model of every member (theta 88 w N^2, u, v 8 w N^2 once and
+        # 80 w N^2 per scalar), summed over the members
+        model = sum(step_model_bytes(m.N, 4, len(m.scalars0)) for m in members)
+        peak, peak_kind = measured_peaks()
+        gbs = model / (ms / steps / 1e3) / 1e9
         return {"value": world * steps / (ms / 1e3), "unit": "ensemble steps/s",
+                "step_model": {"model_bytes_per_step": model, "model_gbs": gbs, "frac_of_peak": gbs / peak,
+                               "peak_kind": peak_kind},
                 "member_steps_per_s": world * len(members) * steps / (ms / 1e3), "ms_per_step": ms / steps,
                 "members": len(members), "passive_scalars": n_scal, "steps": steps, "finite": finite,
                 "gpu_launches_per_step": ens.launches_per_step(),
@@ -639,7 +652,7 @@ def main():
 
     peak, peak_kind = measured_peaks()
     prec = args.precision
-    main_res = measure(args.workload, prec, args.steps, args.warmup, True, True)
+    main_res = measure(args.workload, prec, args.steps, args.warmup, True, True, args.profile_range)
     wb = 4 if prec == "float32" else 8
     N, ns = w["N"], w["scalars"]
     value = world * main_res["steps"] / (main_res["ms"] / 1e3)
