@@ -143,9 +143,36 @@ __device__ __forceinline__ double wavenumber(const KP& kp, int i) {
   return __dmul_rn(__dmul_rn(__dmul_rn((double)m, kp.kval), 2.0), 3.141592653589793116);
 }
 
+// The wavenumber in the arithmetic's precision for the spectral
+// multipliers: float64 (then rounded) in double; in float, the same product
+// in float arithmetic (within an ulp of the rounded float64 value).
+template <typename T>
+__device__ __forceinline__ T wavenumber_t(const KP& kp, int i) {
+  if constexpr (sizeof(T) == 8) {
+    return wavenumber(kp, i);
+  } else {
+    const int m = i <= ((kp.N - 1) >> 1) ? i : i - kp.N;
+    return (float)m * (float)(kp.kval * 6.283185307179586232);
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ T inv_frac(T k2, T alpha, int kind) {
   if (!(k2 > (T)0)) return (T)0;
+  if constexpr (sizeof(T) == 4) {
+    // single precision: the hardware reciprocal square root (about 2 ulp)
+    // instead of correctly rounded square roots and divisions
+    const float r1 = rsqrtf(k2);  // 1 / |k|
+    switch (kind) {
+      case AK_ZERO: return 1.f;
+      case AK_ONE: return r1;
+      case AK_HALF: return rsqrtf(k2 * r1);             // |k|^-1/2
+      case AK_THREEHALF: return r1 * rsqrtf(k2 * r1);   // |k|^-3/2
+      case AK_TWO: return r1 * r1;
+      case AK_MINUSONE: return k2 * r1;
+      default: return powf(k2 * r1, -alpha);
+    }
+  }
   switch (kind) {
     case AK_ZERO: return (T)1;
     case AK_ONE: return (T)1 / sqrt(k2);
@@ -202,7 +229,7 @@ __device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, HA ha
   using C = typename Cplx<T>::type;
   constexpr int N = 1 << LOG2N, G = N / R, H = N / 2, XB = spad_size<R>(N);
   const C* __restrict__ tw = reinterpret_cast<const C*>(kp.tw);
-  const T kx = (T)wavenumber(kp, p);
+  const T kx = wavenumber_t<T>(kp, p);
   const T s_n2 = (T)kp.inv_n2;
   const T dkx = (p == H) ? (T)0 : kx;
   const T nkx = (p == H) ? kx : (T)0;
@@ -213,7 +240,7 @@ __device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, HA ha
     const int iy = j + m * G;
     C h, an;
     ha(m, h, an);
-    const T ky = (T)wavenumber(kp, iy);
+    const T ky = wavenumber_t<T>(kp, iy);
     const T dky = (iy == H) ? (T)0 : ky;
     const T nky = (iy == H) ? ky : (T)0;
     T mm = (T)0;
@@ -270,7 +297,7 @@ template <typename T, int LOG2N, int R, typename HA>
 __device__ __forceinline__ void row_sources(const KP& kp, const RowArgs& a, HA ha, int j, int p) {
   using C = typename Cplx<T>::type;
   constexpr int N = 1 << LOG2N, G = N / R, H = N / 2;
-  const T kx = (T)wavenumber(kp, p);
+  const T kx = wavenumber_t<T>(kp, p);
   const T s_n2 = (T)kp.inv_n2;
   const T dkx = (p == H) ? (T)0 : kx;
   const T nkx = (p == H) ? kx : (T)0;
@@ -280,7 +307,7 @@ __device__ __forceinline__ void row_sources(const KP& kp, const RowArgs& a, HA h
     const int iy = j + m * G;
     C h, an;
     ha(m, h, an);
-    const T ky = (T)wavenumber(kp, iy);
+    const T ky = wavenumber_t<T>(kp, iy);
     const T dky = (iy == H) ? (T)0 : ky;
     const T nky = (iy == H) ? ky : (T)0;
     const T mm = inv_frac<T>(kx * kx + ky * ky, (T)kp.alpha, kp.akind) * s_n2;
