@@ -119,17 +119,20 @@ constexpr int min_blocks_r(int threads) {
                 : min_blocks<T>(threads);
 }
 
-// Row-pass blocks: the pass without the inverse transforms (NFX = 0) and the
-// radix-8 pass that transforms one field at a time (NFX = 1) are held to the
-// radix-4 register budget (64 a thread in single precision, 128 in double),
-// so that more of their blocks fit than of the passes that transform several
-// fields together; the radix-16 one-field pass (256 threads) gets 128
-// registers in single precision, two blocks per SM.
+// NFX of a row pass: 4 or 2 fields transformed together from registers; 6 =
+// two at a time with theta_{s+1} parked in shared memory (its Hermitian part
+// h, or the row itself on the self-paired rows 0 and N/2), so that the
+// transforms hold few registers; 0 = no transforms (the last stage of a step).
+__host__ __device__ constexpr int nfx_fields(int nfx) { return nfx == 6 ? 2 : nfx; }
+__host__ __device__ constexpr bool nfx_park(int nfx) { return nfx == 6; }
+
+// Row-pass blocks: the passes without inverse transforms (NFX = 0) and the
+// parked passes (NFX = 6) are held to the radix-4 register budget (64 a
+// thread in single precision, 128 in double), so that more of their blocks
+// fit than of the passes that transform fields from registers.
 template <typename T, int R, int NFX>
 constexpr int row_min_blocks(int threads) {
-  // radix 16 one field at a time: 128 registers (two 256-thread blocks per SM)
-  return (NFX == 1 && R == 16) ? min_blocks<T>(threads)
-                               : (NFX <= 1 ? min_blocks_r<T, 4>(threads) : min_blocks_r<T, R>(threads));
+  return (NFX == 0 || nfx_park(NFX)) ? min_blocks_r<T, 4>(threads) : min_blocks_r<T, R>(threads);
 }
 
 __device__ __forceinline__ int mode_abs(int i, int N) { return i <= (N >> 1) ? i : N - i; }
@@ -289,40 +292,6 @@ __device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, HA ha
   }
 }
 
-// Mean-gradient scalar sources S^ = -N^2 (gx X_u + gy X_v) = -(gx u^ + gy v^)
-// on rows p (kx >= 0) from the spectra X_u, X_v of the u and v fields (the
-// expressions of row_fields), for the n_src scalars that carry one; used by
-// the one-field-at-a-time pass, where u and v are not in the same batch.
-template <typename T, int LOG2N, int R, typename HA>
-__device__ __forceinline__ void row_sources(const KP& kp, const RowArgs& a, HA ha, int j, int p) {
-  using C = typename Cplx<T>::type;
-  constexpr int N = 1 << LOG2N, G = N / R, H = N / 2;
-  const T kx = wavenumber_t<T>(kp, p);
-  const T s_n2 = (T)kp.inv_n2;
-  const T dkx = (p == H) ? (T)0 : kx;
-  const T nkx = (p == H) ? kx : (T)0;
-  const T n2 = (T)1 / s_n2;
-#pragma unroll
-  for (int m = 0; m < R; ++m) {
-    const int iy = j + m * G;
-    C h, an;
-    ha(m, h, an);
-    const T ky = wavenumber_t<T>(kp, iy);
-    const T dky = (iy == H) ? (T)0 : ky;
-    const T nky = (iy == H) ? ky : (T)0;
-    const T mm = inv_frac<T>(kx * kx + ky * ky, (T)kp.alpha, kp.akind) * s_n2;
-    const C qu = cadd(cscale(h, dky), cscale(an, nky));
-    const C qv = cadd(cscale(h, dkx), cscale(an, nkx));
-    const C Xu = mkc<C>(mm * qu.y, -mm * qu.x);
-    const C Xv = mkc<C>(-mm * qv.y, mm * qv.x);
-    for (int sidx = 0; sidx < a.n_src; ++sidx) {
-      C* so = reinterpret_cast<C*>(a.src_out[sidx]);
-      const T gx = (T)a.gx[sidx], gy = (T)a.gy[sidx];
-      so[(size_t)p * N + iy] = mkc<C>(-n2 * (gx * Xu.x + gy * Xv.x), -n2 * (gx * Xu.y + gy * Xv.y));
-    }
-  }
-}
-
 // Row pass.  DEPTH: how many of the R element chunks of a thread (chunk m =
 // the elements iy = j + m G) have their theta_n / acc values prefetched with
 // cp.async ahead of use; the first DEPTH chunks are requested before the
@@ -338,12 +307,13 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
   const int grp = threadIdx.x / G;
   const int j = threadIdx.x - grp * G;
   constexpr int XB = spad_size<R>(N);  // one exchange buffer
-  constexpr int NB = NFX > 0 ? NFX : 1;  // exchange buffers per group
+  constexpr int NFT = nfx_fields(NFX);              // fields transformed together
+  constexpr int NB = NFX > 0 ? NFT : 1;            // exchange buffers per group
   C* wbuf = smem + (size_t)grp * NB * XB;
   // prefetch staging: DEPTH chunks x 4 slots (theta_n e1/e2, acc e1/e2) x G
   const int rpc = a.rpc > 0 ? a.rpc : RPC;  // launch shape (autotuned), <= RPC
   C* pf = smem + (size_t)rpc * NB * XB + (size_t)grp * (DEPTH * 4 * G);
-  static_assert(NFX != 1 || DEPTH * 4 * G >= 2 * N, "the one-field pass keeps h and an in the staging slots");
+  static_assert(!nfx_park(NFX) || DEPTH * 4 * G >= N, "the parked passes keep theta_{s+1} in the staging slots");
   const int p_raw = tile * rpc + grp;
   const bool valid = p_raw <= H;
   const int p = valid ? p_raw : H;
@@ -563,8 +533,9 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
   if (!a.do_p1) return;
 
   // Rows 0 and N/2 pair with themselves: e2 = (p, N - iy) is owned by another
-  // thread of the group, so its new value is exchanged through shared memory.
-  if (a.rmode != RM_P1) {
+  // thread of the group, so its new value is exchanged through shared memory
+  // (the parked passes read it from the parked row instead).
+  if (a.rmode != RM_P1 && !nfx_park(NFX)) {
     __syncthreads();
     if (!pair) {
 #pragma unroll
@@ -578,55 +549,55 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
   }
   // Hermitian and anti-Hermitian parts of theta_{s+1} at (p, iy), h = (t1 +
   // conj t2) / 2 and an = (t1 - conj t2) / 2, for the transforms: from the
-  // registers, or -- in the one-field-at-a-time pass, which must fit in 64
-  // registers -- computed once into this group's prefetch staging slots
-  // (free once the update has consumed them; indices j + m G and N + j + m G
-  // are this thread's own slots, so no barrier is needed).
+  // registers, or -- in the parked passes, which must fit in 64 registers --
+  // from this group's prefetch staging slots, free once the update has
+  // consumed them.  On the paired rows an enters only at iy = N/2 (through
+  // nky; nkx is zero there), so h alone is parked plus that one value.
   C* hs = pf;
-  if constexpr (NFX == 1) {
+  C anH = mkc<C>(0, 0);  // an at iy = N/2 (element m = R/2 of thread 0)
+  if constexpr (nfx_park(NFX)) {
+    // park h (paired rows) or the row itself (rows 0 and N/2) in this
+    // thread's own staging slots j + m G; the self-paired rows then read the
+    // mirrored element of another thread, hence the barrier
 #pragma unroll
-    for (int m = 0; m < R; ++m) {
-      hs[j + m * G] = cscale(cadd(t1[m], cconj(t2[m])), (T)0.5);
-      hs[N + j + m * G] = cscale(csub(t1[m], cconj(t2[m])), (T)0.5);
-    }
+    for (int m = 0; m < R; ++m) hs[j + m * G] = pair ? cscale(cadd(t1[m], cconj(t2[m])), (T)0.5) : t1[m];
+    anH = cscale(csub(t1[R / 2], cconj(t2[R / 2])), (T)0.5);
+    __syncthreads();
   }
   auto ha_reg = [&](int m, C& h, C& an) {
     h = cscale(cadd(t1[m], cconj(t2[m])), (T)0.5);
     an = cscale(csub(t1[m], cconj(t2[m])), (T)0.5);
   };
   auto ha_smem = [&](int m, C& h, C& an) {
-    h = hs[j + m * G];
-    an = hs[N + j + m * G];
-  };
-  auto fields = [&](auto ha) {
-    // (the passes that transform u and v together write the sources there)
-    if constexpr (NFX == 1) {
-      if (a.fmode == FM_VEL && a.n_src > 0 && valid) row_sources<T, LOG2N, R>(kp, a, ha, j, p);
+    const int iy = j + m * G;
+    if (pair) {  // the anti-Hermitian part enters only at the Nyquist element
+      h = hs[iy];
+      an = iy == H ? anH : mkc<C>(0, 0);
+    } else {
+      const C x1 = hs[iy], x2 = hs[(N - iy) & (N - 1)];
+      h = cscale(cadd(x1, cconj(x2)), (T)0.5);
+      an = cscale(csub(x1, cconj(x2)), (T)0.5);
     }
-    // Inverse transforms along y of the multiplied Hermitian projections,
-    // NFX fields at a time.
+  };
+  // Inverse transforms along y of the multiplied Hermitian projections, NFT
+  // fields at a time (row_fields<.., NF> exchanges through NF <= NB buffers;
+  // the batch with u and v also writes the mean-gradient sources).
+  static_assert(NFT == 2 || NFT == 4, "row passes with transforms take two or four fields at a time");
+  auto fields = [&](auto ha) {
     if (a.fmode == FM_THETA) {
-      if constexpr (NFX >= 4) {
+      if constexpr (NFT == 4) {
         row_fields<T, LOG2N, R, 4>(kp, a, ha, 0, j, p, valid, wbuf);
-      } else if constexpr (NFX == 2) {
+      } else {
         row_fields<T, LOG2N, R, 2>(kp, a, ha, 0, j, p, valid, wbuf);
         row_fields<T, LOG2N, R, 2>(kp, a, ha, 2, j, p, valid, wbuf);
-      } else {
-#pragma unroll 1
-        for (int f = 0; f < 4; ++f) row_fields<T, LOG2N, R, 1>(kp, a, ha, f, j, p, valid, wbuf);
       }
     } else if (a.fmode == FM_PHYS1) {
       row_fields<T, LOG2N, R, 1>(kp, a, ha, 0, j, p, valid, wbuf);
     } else {
-      if constexpr (NFX >= 2) {
-        row_fields<T, LOG2N, R, 2>(kp, a, ha, 0, j, p, valid, wbuf);
-      } else {
-#pragma unroll 1
-        for (int f = 0; f < 2; ++f) row_fields<T, LOG2N, R, 1>(kp, a, ha, f, j, p, valid, wbuf);
-      }
+      row_fields<T, LOG2N, R, 2>(kp, a, ha, 0, j, p, valid, wbuf);
     }
   };
-  if constexpr (NFX == 1) fields(ha_smem);
+  if constexpr (nfx_park(NFX)) fields(ha_smem);
   else fields(ha_reg);
   }
 }

@@ -61,24 +61,23 @@ constexpr int col_nbuf() {
          : (size_t)pairs_per_cta<T, L>() * 4 * ColBuf<(1 << L), col_radix<T, L>()>::SZ *
                        sizeof(typename Cplx<T>::type) <= 150 * 1024 ? 4 : 2;
 }
-// Exchange buffers of the row pass: four (the theta fields transform
-// together) when they fit in 150 KB, else two (two rounds); two for a
-// radix-4 or radix-16 row pass.
+// Fields the row pass transforms together (row_body's NFX): four (one
+// exchange buffer each) when their buffers fit in 150 KB, else two (two
+// rounds); two for a radix-4 or radix-16 row pass.  FP32 at N = 4096 takes
+// two at a time with theta_{s+1} parked in shared memory (NFX = 6) at 64
+// registers, two 512-thread blocks per SM (measured against four fields from
+// registers at one block per SM: theta stage pass 332 -> 289 us; scalar
+// stage pass 221 -> 202 us against one field at a time).
 template <typename T, int L>
 constexpr int row_nfx() {
+  if (sizeof(T) == 4 && L == 12) return 6;
   return row_radix<T, L>() != 8 ? 2
          : (size_t)rows_per_cta<T, L>() * 4 * spad_size<row_radix<T, L>()>(1 << L) * sizeof(typename Cplx<T>::type) <=
                    150 * 1024 ? 4 : 2;
 }
-// Scalar stage passes (two fields: s_x, s_y) at N = 4096 in float transform
-// one field at a time at 64 registers, two 512-thread blocks per SM
-// (measured: 258 -> 222 us per launch; the theta passes with four fields
-// were slower that way, 354 -> 394 us, and keep row_nfx).
-template <typename T, int L>
-constexpr int row_nfx_scalar() { return (sizeof(T) == 4 && L == 12) ? 1 : row_nfx<T, L>(); }
 template <typename T, int L, int NFX = row_nfx<T, L>()>
 constexpr size_t row_base_smem() {
-  return (size_t)rows_per_cta<T, L>() * (NFX > 0 ? NFX : 1) * spad_size<row_radix<T, L>()>(1 << L) *
+  return (size_t)rows_per_cta<T, L>() * (NFX > 0 ? nfx_fields(NFX) : 1) * spad_size<row_radix<T, L>()>(1 << L) *
          sizeof(typename Cplx<T>::type);
 }
 template <typename T, int L>
@@ -105,9 +104,9 @@ constexpr int row_depth() {
     const int o = row_occupancy<T, L, NFX>(d);
     if (o >= occ && o > 0) { occ = o; best = d; }
   }
-  // the one-field pass keeps h and an in the staging slots (2 N elements)
-  if (NFX == 1)
-    while (best < R && best * 4 * row_group<T, L>() < 2 * (1 << L)) best *= 2;
+  // the parked passes keep theta_{s+1} in the staging slots (N elements)
+  if (nfx_park(NFX))
+    while (best < R && best * 4 * row_group<T, L>() < (1 << L)) best *= 2;
   return best;
 }
 template <typename T, int L, int NFX = row_nfx<T, L>()>
@@ -205,12 +204,6 @@ cudaError_t launch_row_t(const KP& kp, const RowArgs& a, cudaStream_t st) {
                       dim3((N / 2 + 1 + RPCX - 1) / RPCX), dim3(RPCX * rowx_group<T, L>()),
                       rowx_smem<T, L>(rowx_depth<T, L>()), st, kp, ax);
   }
-  if constexpr (row_nfx_scalar<T, L>() != row_nfx<T, L>()) {
-    constexpr int NS = row_nfx_scalar<T, L>();
-    if (a.fmode == FM_SCAL && a.rmode == RM_STAGE)
-      return launch_pdl(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L, NS>(), NS>, dim3(grid),
-                        dim3(rpc * row_group<T, L>()), row_smem<T, L, NS>() / RPC * rpc, st, kp, a);
-  }
   return launch_pdl(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>, dim3(grid),
                     dim3(rpc * row_group<T, L>()), row_smem<T, L>() / RPC * rpc, st, kp, a);
 }
@@ -234,12 +227,6 @@ cudaError_t set_attrs_t() {
   cudaError_t e = cudaFuncSetAttribute(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem<T, L>());
   if (e != cudaSuccess) return e;
-  if constexpr (row_nfx_scalar<T, L>() != row_nfx<T, L>()) {
-    constexpr int NS = row_nfx_scalar<T, L>();
-    e = cudaFuncSetAttribute(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L, NS>(), NS>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem<T, L, NS>());
-    if (e != cudaSuccess) return e;
-  }
   e = cudaFuncSetAttribute(k_row<T, L, rowx_radix<T, L>(), rowx_rpc<T, L>(), rowx_depth<T, L>(), 0>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rowx_smem<T, L>(rowx_depth<T, L>()));
   if (e != cudaSuccess) return e;

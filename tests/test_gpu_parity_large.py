@@ -6,8 +6,9 @@ Variants covered here (launch shapes are chosen per N and precision):
   * FP64 radix-4 row pass at N = 512, 1024, 2048 (forced, damped IF-RK4);
   * FP32 radix-16 column pass (one or two column pairs per block), the
     radix-8 row pass and the last-stage row pass at N = 2048 and 4096;
-  * the scalar row and column passes at N = 256 and 512 (FP64) and 1024
-    (FP32), with and without a mean-gradient source;
+  * the scalar row and column passes at N = 256 and 512 (FP64), 1024 and
+    4096 (FP32; at 4096 the stage passes run at 64 registers with theta_{s+1}
+    parked in shared memory), with and without a mean-gradient source;
   * the mean-gradient source S = -G.u (no reference counterpart: the oracle
     evaluates it as fft2(-(G_x u + G_y v)) from the velocity of the new theta,
     frozen over the scalar's RK stages as the reference freezes u, v,
@@ -159,7 +160,8 @@ def test_fp32_large_passes_vs_fp64_oracle(P, N, alpha):
     assert err < 2e-5, err
 
 
-@pytest.mark.parametrize("N,prec,tol", [(256, "float64", 1e-11), (512, "float64", 1e-11), (1024, "float32", 2e-5)])
+@pytest.mark.parametrize("N,prec,tol", [(256, "float64", 1e-11), (512, "float64", 1e-11), (1024, "float32", 2e-5),
+                                        (4096, "float32", 2e-5)])
 def test_scalar_passes_vs_oracle(P, N, prec, tol):
     scal = [(1e-4, (1.0, 0.0)), (5e-4, None)]
     st, sto = run_pair(P, N, 1.0, prec, 2, 2e-4, 80 + N, scalars=scal)
