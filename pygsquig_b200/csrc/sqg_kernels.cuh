@@ -217,26 +217,30 @@ __device__ __forceinline__ int ring_ord(const RowTab& rt, int iy) {
 // (the reference's .real projections, operators.py:15-34, 76-97, 101-130).
 enum FieldKind { FK_U = 0, FK_V = 1, FK_DX = 2, FK_DY = 3, FK_ID = 4 };
 
-__device__ __forceinline__ int field_kind(int fmode, int f) {
-  if (fmode == FM_THETA || fmode == FM_VEL) return f;  // u, v, dx, dy
-  if (fmode == FM_PHYS1) return FK_ID;
-  return FK_DX + f;                                    // scalar: dx, dy
+// Field sets a row_fields call transforms together (fixed at compile time, so
+// that each element forms only the spectra of its own kinds): u and v; the
+// gradient (dx, dy); all four (u, v, dx, dy); the field itself.
+enum FieldSet { FS_UV = 0, FS_GRAD = 1, FS_ALL = 2, FS_ID = 3 };
+__host__ __device__ constexpr int fs_fields(int fs) { return fs == FS_ALL ? 4 : (fs == FS_ID ? 1 : 2); }
+__host__ __device__ constexpr int fs_kind(int fs, int f) {
+  return fs == FS_ID ? FK_ID : (fs == FS_GRAD ? FK_DX + f : f);
 }
 
-// Fields f0 .. f0+NF-1 of the row pair's mode: form their spectra from
+// The fields of set FS of the row pair's mode: form their spectra from
 // theta_{s+1} at (p, iy) / (N-p, N-iy), transform them together along y and
-// write xh[f][p][:].
-template <typename T, int LOG2N, int R, int NF, typename HA>
+// write xh[f0 + f][p][:].
+template <typename T, int LOG2N, int R, int FS, typename HA>
 __device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, HA ha, int f0, int j, int p, bool valid,
                                            typename Cplx<T>::type* wbuf) {
   using C = typename Cplx<T>::type;
   constexpr int N = 1 << LOG2N, G = N / R, H = N / 2, XB = spad_size<R>(N);
+  constexpr int NF = fs_fields(FS);
+  constexpr bool uv = FS == FS_UV || FS == FS_ALL;  // u and v: the multiplier |k|^-alpha
   const C* __restrict__ tw = reinterpret_cast<const C*>(kp.tw);
   const T kx = wavenumber_t<T>(kp, p);
   const T s_n2 = (T)kp.inv_n2;
   const T dkx = (p == H) ? (T)0 : kx;
   const T nkx = (p == H) ? kx : (T)0;
-  const bool uv = (a.fmode == FM_THETA || a.fmode == FM_VEL);
   C V[NF][R];
 #pragma unroll
   for (int m = 0; m < R; ++m) {
@@ -247,10 +251,10 @@ __device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, HA ha
     const T dky = (iy == H) ? (T)0 : ky;
     const T nky = (iy == H) ? ky : (T)0;
     T mm = (T)0;
-    if (uv) mm = inv_frac<T>(kx * kx + ky * ky, (T)kp.alpha, kp.akind) * s_n2;
+    if constexpr (uv) mm = inv_frac<T>(kx * kx + ky * ky, (T)kp.alpha, kp.akind) * s_n2;
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
-      const int kind = field_kind(a.fmode, f0 + f);
+      const int kind = fs_kind(FS, f);
       C X;
       if (kind == FK_U) {
         const C q = cadd(cscale(h, dky), cscale(an, nky));
@@ -267,8 +271,8 @@ __device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, HA ha
       }
       V[f][m] = X;
     }
-    if constexpr (NF >= 2) {
-      if (uv && f0 == 0 && a.n_src > 0 && valid) {
+    if constexpr (uv) {
+      if (a.n_src > 0 && valid) {
         // S^ = -N^2 (gx X_u + gy X_v): the mean-gradient scalar sources, from
         // the u and v spectra of this batch
         const T n2 = (T)1 / s_n2;
@@ -586,15 +590,17 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
   auto fields = [&](auto ha) {
     if (a.fmode == FM_THETA) {
       if constexpr (NFT == 4) {
-        row_fields<T, LOG2N, R, 4>(kp, a, ha, 0, j, p, valid, wbuf);
+        row_fields<T, LOG2N, R, FS_ALL>(kp, a, ha, 0, j, p, valid, wbuf);
       } else {
-        row_fields<T, LOG2N, R, 2>(kp, a, ha, 0, j, p, valid, wbuf);
-        row_fields<T, LOG2N, R, 2>(kp, a, ha, 2, j, p, valid, wbuf);
+        row_fields<T, LOG2N, R, FS_UV>(kp, a, ha, 0, j, p, valid, wbuf);
+        row_fields<T, LOG2N, R, FS_GRAD>(kp, a, ha, 2, j, p, valid, wbuf);
       }
     } else if (a.fmode == FM_PHYS1) {
-      row_fields<T, LOG2N, R, 1>(kp, a, ha, 0, j, p, valid, wbuf);
+      row_fields<T, LOG2N, R, FS_ID>(kp, a, ha, 0, j, p, valid, wbuf);
+    } else if (a.fmode == FM_VEL) {
+      row_fields<T, LOG2N, R, FS_UV>(kp, a, ha, 0, j, p, valid, wbuf);
     } else {
-      row_fields<T, LOG2N, R, 2>(kp, a, ha, 0, j, p, valid, wbuf);
+      row_fields<T, LOG2N, R, FS_GRAD>(kp, a, ha, 0, j, p, valid, wbuf);
     }
   };
   if constexpr (nfx_park(NFX)) fields(ha_smem);
