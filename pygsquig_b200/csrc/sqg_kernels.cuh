@@ -406,13 +406,16 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
       const C* slot = pf + (size_t)(m % DEPTH) * 4 * G + j;
       const double kyd = wavenumber(kp, iy);
       const double k2d = kxd * kxd + kyd * kyd;
-      // diagonal linear operator in float64
-      double Ld;
-      if (scal) {
-        Ld = -a.kappa * k2d;
-      } else {
-        Ld = -kp.nu_s * kpow(k2d, kp.ps) - kp.nu_d * kpow(k2d, kp.pd);
-        if (my <= rt.dragmax) Ld -= kp.mu;
+      // diagonal linear operator in float64 (the integrating-factor form's
+      // last stage, th_{n+1} = acc + dt/6 k, does not use it)
+      double Ld = 0.0;
+      if (explicit_lin || s < 4) {
+        if (scal) {
+          Ld = -a.kappa * k2d;
+        } else {
+          Ld = -kp.nu_s * kpow(k2d, kp.ps) - kp.nu_d * kpow(k2d, kp.pd);
+          if (my <= rt.dragmax) Ld -= kp.mu;
+        }
       }
       const T dmask = (my <= rt.dmax) ? (T)1 : (T)0;
       C J1 = v[m];
@@ -470,7 +473,7 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
         const T Lt = (T)Ld;
         k1v = cadd(k1v, cscale(xs1, Lt));
         k2v = cadd(k2v, cscale(xs2, Lt));
-      } else {
+      } else if (s < 4) {
         const double x = Ld * (0.5 * dt);
         const double Ed = x < -745.0 ? 0.0 : exp(x);
         E = (T)Ed;
@@ -732,7 +735,9 @@ __device__ void ring_reduce(const KP& kp, const ColArgs& a);
 // Column pass.  NBUF = 4: all four fields of the column pairs are fetched at
 // once (round-2 copies land while round 1 computes); NBUF = 2: two rounds of
 // two fields (large N in float64, where four buffers do not fit).
-template <typename T, int LOG2N, int R, int NP, int NBUF>
+// CMX >= 0: an instance compiled for that column mode alone (the other
+// modes' branches fold away); -1: every mode, chosen by a.cmode at run time.
+template <typename T, int LOG2N, int R, int NP, int NBUF, int CMX = -1>
 __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int tile, int ntiles) {
   using C = typename Cplx<T>::type;
   constexpr int N = 1 << LOG2N;
@@ -741,7 +746,8 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
   constexpr int SZ = ColBuf<N, R>::SZ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* smem = reinterpret_cast<C*>(smem_raw);
-  if (a.ring_cta && tile == ntiles - 1) {
+  const int cmode = CMX >= 0 ? CMX : a.cmode;
+  if ((CMX < 0 || CMX == CM_THETA) && a.ring_cta && tile == ntiles - 1) {
     ring_reduce<T, LOG2N>(kp, a);
     return;
   }
@@ -757,7 +763,7 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
   const size_t fstride = (size_t)(H + 1) * N;
   C v[R];
 
-  if (a.cmode == CM_VEL && !a.out1) {
+  if (cmode == CM_VEL && !a.out1) {
     // u + i v for the scalar passes, column-pair-major (uv_index): both
     // fields transformed together, one 16-byte (float) or two 16-byte
     // (double) stores per thread and row
@@ -779,8 +785,8 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
     }
     return;
   }
-  if (a.cmode == CM_VEL || a.cmode == CM_PHYS1) {
-    const int nf = a.cmode == CM_VEL ? 2 : 1;
+  if (cmode == CM_VEL || cmode == CM_PHYS1) {
+    const int nf = cmode == CM_VEL ? 2 : 1;
     for (int f = 0; f < nf; ++f) col_fetch<T, LOG2N, R, NP, NBUF>(xh + f * fstride, y0, f, smem, np);
     cp_async_commit();
     cp_async_wait<0>();
@@ -790,7 +796,7 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
       col_first_load<T, LOG2N, R>(b, j, v);
       fft_group<T, LOG2N, R, +1>(v, b, j, tw);
       // v[m] = f(x, ya) + i f(x, ya+1), x = j + m G
-      if (a.cmode == CM_PHYS1 || a.out1) {
+      if (cmode == CM_PHYS1 || a.out1) {
         T* o = reinterpret_cast<T*>(f == 0 ? a.out0 : a.out1);
 #pragma unroll
         for (int m = 0; m < R; ++m) {
@@ -817,13 +823,13 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
   C W[R];
 #pragma unroll
   for (int m = 0; m < R; ++m) W[m] = mkc<C>(0, 0);
-  if (NBUF != 4 && a.cmode == CM_SCALV) return;  // not supported (the host never asks for it)
-  const int nround = (a.cmode == CM_THETA || a.cmode == CM_SCALV) ? 2 : (a.cmode == CM_SCAL ? 1 : 0);
-  const int fa0 = 0, fb0 = a.cmode == CM_THETA ? 2 : 1, fa1 = 1, fb1 = 3;
+  if (NBUF != 4 && cmode == CM_SCALV) return;  // not supported (the host never asks for it)
+  const int nround = (cmode == CM_THETA || cmode == CM_SCALV) ? 2 : (cmode == CM_SCAL ? 1 : 0);
+  const int fa0 = 0, fb0 = cmode == CM_THETA ? 2 : 1, fa1 = 1, fb1 = 3;
   if (nround > 0) {
     // CM_SCALV: buffers (u, s_x, v, s_y) -- u, v from theta's xh, s_x, s_y from xh2
-    const C* xb = a.cmode == CM_SCALV ? reinterpret_cast<const C*>(a.xh2) : xh;
-    const int fb0s = a.cmode == CM_SCALV ? 0 : fb0, fb1s = a.cmode == CM_SCALV ? 1 : fb1;
+    const C* xb = cmode == CM_SCALV ? reinterpret_cast<const C*>(a.xh2) : xh;
+    const int fb0s = cmode == CM_SCALV ? 0 : fb0, fb1s = cmode == CM_SCALV ? 1 : fb1;
     col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa0 * fstride, y0, 0, smem, np);
     col_fetch<T, LOG2N, R, NP, NBUF>(xb + fb0s * fstride, y0, 1, smem, np);
     if (NBUF == 4 && nround == 2) {
@@ -832,7 +838,7 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
     }
     cp_async_commit();
   }
-  if (a.cmode == CM_FWD) {
+  if (cmode == CM_FWD) {
     const T* f = reinterpret_cast<const T*>(a.in_real);
 #pragma unroll
     for (int m = 0; m < R; ++m) {
@@ -854,7 +860,7 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
       W[m].x = V[0][m].x * V[1][m].x + V[2][m].x * V[3][m].x;
       W[m].y = V[0][m].y * V[1][m].y + V[2][m].y * V[3][m].y;
     }
-    if (a.cmode == CM_SCALV && a.out0) {  // u + i v for the later stages (column-pair-major)
+    if (cmode == CM_SCALV && a.out0) {  // u + i v for the later stages (column-pair-major)
       C* o = reinterpret_cast<C*>(a.out0);
 #pragma unroll
       for (int m = 0; m < R; ++m)
@@ -883,7 +889,7 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
       col_first_load<T, LOG2N, R>(gbuf, j, V[0]);
       col_first_load<T, LOG2N, R>(gbuf + SZ, j, V[1]);
       fft_multi<T, LOG2N, R, +1, 2>(V, gbuf, SZ, j, tw);
-      if (a.cmode == CM_THETA) {
+      if (cmode == CM_THETA) {
 #pragma unroll
         for (int m = 0; m < R; ++m) {
           W[m].x += V[0][m].x * V[1][m].x;
@@ -904,7 +910,7 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
       }
     }
   }
-  if (!(NBUF == 4 && nround == 2) && a.cmode == CM_THETA && a.in_real) {  // physical-space source: J - src
+  if (!(NBUF == 4 && nround == 2) && cmode == CM_THETA && a.in_real) {  // physical-space source: J - src
     const T* f = reinterpret_cast<const T*>(a.in_real);
 #pragma unroll
     for (int m = 0; m < R; ++m) {
@@ -1028,11 +1034,11 @@ k_row(KP kp, RowArgs a) {
   row_body<T, LOG2N, R, RPC, DEPTH, NFX>(kp, a, blockIdx.x);
 }
 
-template <typename T, int LOG2N, int R, int NP, int NBUF>
+template <typename T, int LOG2N, int R, int NP, int NBUF, int CMX = -1>
 __global__ void __launch_bounds__(NP * ((1 << LOG2N) / R), min_blocks_r<T, R>(NP * ((1 << LOG2N) / R)))
 k_col(KP kp, ColArgs a) {
   pdl_wait();
-  col_body<T, LOG2N, R, NP, NBUF>(kp, a, blockIdx.x, gridDim.x);
+  col_body<T, LOG2N, R, NP, NBUF, CMX>(kp, a, blockIdx.x, gridDim.x);
 }
 
 // Batched forms: the member's parameters come from device arrays; members
