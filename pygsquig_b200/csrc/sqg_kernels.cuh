@@ -43,6 +43,9 @@ struct RowTab {
 
 enum FieldMode { FM_THETA = 0, FM_VEL = 1, FM_PHYS1 = 2, FM_SCAL = 3 };
 enum RowMode { RM_P1 = 0, RM_STAGE = 1, RM_RHS = 2, RM_SPEC = 3 };
+// Row-pass instances: one that reads its modes from the arguments, and the
+// stage passes of theta and of the scalars compiled for their modes alone.
+enum RowInst { RI_ANY = 0, RI_THETA_STAGE = 1, RI_SCAL_STAGE = 2 };
 enum AlphaKind { AK_GENERAL = 0, AK_ZERO = 1, AK_ONE = 2, AK_HALF = 3, AK_THREEHALF = 4, AK_TWO = 5, AK_MINUSONE = 6 };
 enum StageWrite { SW_NONE = 0, SW_FULL = 1, SW_RING = 2 };
 
@@ -300,8 +303,11 @@ __device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, HA ha
 // the elements iy = j + m G) have their theta_n / acc values prefetched with
 // cp.async ahead of use; the first DEPTH chunks are requested before the
 // forward FFT of the J row, so their latency hides behind it.
-template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
+template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX, int RI = RI_ANY>
 __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int tile) {
+  // modes fixed by the instance (RI), else read from the arguments
+  const int rmode = RI == RI_ANY ? a.rmode : RM_STAGE;
+  const int fmode = RI == RI_THETA_STAGE ? FM_THETA : (RI == RI_SCAL_STAGE ? FM_SCAL : a.fmode);
   using C = typename Cplx<T>::type;
   constexpr int N = 1 << LOG2N;
   constexpr int G = N / R;
@@ -334,7 +340,7 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
   C t1[R];  // theta_{s+1} (or theta_in) at e1 = (p, iy)
   C t2[R];  // theta_{s+1} at e2 = (pp, N - iy)
 
-  if (a.rmode == RM_P1) {
+  if (rmode == RM_P1) {
     const C* th = reinterpret_cast<const C*>(a.th_n);
 #pragma unroll
     for (int m = 0; m < R; ++m) {
@@ -346,8 +352,8 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
   } else {
     // stage pass: request this thread's theta_n / acc elements of the first
     // DEPTH chunks (own slots only, so no barrier is needed to consume them)
-    const bool pf_th = a.rmode == RM_STAGE && a.stage <= 3;
-    const bool pf_acc = a.rmode == RM_STAGE && a.stage >= 2;
+    const bool pf_th = rmode == RM_STAGE && a.stage <= 3;
+    const bool pf_acc = rmode == RM_STAGE && a.stage >= 2;
     const C* pth = reinterpret_cast<const C*>(a.th_n);
     const C* pacc = reinterpret_cast<const C*>(a.acc);
     auto issue = [&](int m) {
@@ -372,7 +378,7 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
     for (int m = 0; m < R; ++m) v[m] = jh[(size_t)p * N + j + m * G];
     fft_group<T, LOG2N, R, -1>(v, wbuf, j, tw);
     // v[m] = J^(p, iy) ; J^(pp, N - iy) = conj(v[m])
-    if (a.rmode == RM_SPEC) {
+    if (rmode == RM_SPEC) {
       // forward transform of a real field: rows p and N - p of its spectrum
       C* out = reinterpret_cast<C*>(a.rhs_out);
       if (valid) {
@@ -386,7 +392,7 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
       return;
     }
     const int s = a.stage;
-    const bool scal = a.fmode == FM_SCAL;
+    const bool scal = fmode == FM_SCAL;
     const C* st_in = reinterpret_cast<const C*>(s == 1 ? a.th_n : a.st_in);
     C* acc = reinterpret_cast<C*>(a.acc);
     C* st_out = reinterpret_cast<C*>(a.st_out);
@@ -445,7 +451,7 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
         n1 = cadd(n1, extra[e1]);
         if (pair) n2 = cadd(n2, extra[e2]);
       }
-      if (a.rmode == RM_RHS) {
+      if (rmode == RM_RHS) {
         // core RHS (solver.py:28-58): advection + solver hyperviscosity only
         const C x1 = st_in[e1];
         const T Ls = (T)(-kp.nu_s * kpow(k2d, kp.ps));
@@ -542,7 +548,7 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
   // Rows 0 and N/2 pair with themselves: e2 = (p, N - iy) is owned by another
   // thread of the group, so its new value is exchanged through shared memory
   // (the parked passes read it from the parked row instead).
-  if (a.rmode != RM_P1 && !nfx_park(NFX)) {
+  if (rmode != RM_P1 && !nfx_park(NFX)) {
     __syncthreads();
     if (!pair) {
 #pragma unroll
@@ -591,16 +597,16 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
   // the batch with u and v also writes the mean-gradient sources).
   static_assert(NFT == 2 || NFT == 4, "row passes with transforms take two or four fields at a time");
   auto fields = [&](auto ha) {
-    if (a.fmode == FM_THETA) {
+    if (fmode == FM_THETA) {
       if constexpr (NFT == 4) {
         row_fields<T, LOG2N, R, FS_ALL>(kp, a, ha, 0, j, p, valid, wbuf);
       } else {
         row_fields<T, LOG2N, R, FS_UV>(kp, a, ha, 0, j, p, valid, wbuf);
         row_fields<T, LOG2N, R, FS_GRAD>(kp, a, ha, 2, j, p, valid, wbuf);
       }
-    } else if (a.fmode == FM_PHYS1) {
+    } else if (fmode == FM_PHYS1) {
       row_fields<T, LOG2N, R, FS_ID>(kp, a, ha, 0, j, p, valid, wbuf);
-    } else if (a.fmode == FM_VEL) {
+    } else if (fmode == FM_VEL) {
       row_fields<T, LOG2N, R, FS_UV>(kp, a, ha, 0, j, p, valid, wbuf);
     } else {
       row_fields<T, LOG2N, R, FS_GRAD>(kp, a, ha, 0, j, p, valid, wbuf);
@@ -1027,11 +1033,11 @@ __device__ void ring_reduce(const KP& kp, const ColArgs& a) {
 
 namespace sqg {
 // ---- kernels: one plan, or a batch of members (member = blockIdx.y) ----
-template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX>
+template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX, int RI = RI_ANY>
 __global__ void __launch_bounds__(RPC * ((1 << LOG2N) / R), row_min_blocks<T, R, NFX>(RPC * ((1 << LOG2N) / R)))
 k_row(KP kp, RowArgs a) {
   pdl_wait();
-  row_body<T, LOG2N, R, RPC, DEPTH, NFX>(kp, a, blockIdx.x);
+  row_body<T, LOG2N, R, RPC, DEPTH, NFX, RI>(kp, a, blockIdx.x);
 }
 
 template <typename T, int LOG2N, int R, int NP, int NBUF, int CMX = -1>

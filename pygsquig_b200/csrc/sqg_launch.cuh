@@ -191,26 +191,42 @@ template <typename T> int multi_col_tiles(int log2n);
 // size of the CTAs change.
 // The row and column passes are launched with programmatic dependent launch
 // (pdl.cuh): the next pass's launch overlaps the tail of the current one.
-template <typename T, int L>
-cudaError_t launch_row_t(const KP& kp, const RowArgs& a, cudaStream_t st) {
+// The stage passes of theta and of the scalars run instances compiled for
+// their modes alone (RowInst: N = 4096 FP32 theta stage pass 290 -> 282 us,
+// scalar stage pass 193 -> 184 us); the other row passes run the instance
+// that reads its modes from the arguments.
+constexpr int row_inst(int rmode, int fmode) {
+  return rmode != RM_STAGE ? RI_ANY : (fmode == FM_THETA ? RI_THETA_STAGE : (fmode == FM_SCAL ? RI_SCAL_STAGE : RI_ANY));
+}
+template <typename T, int L, int RI>
+cudaError_t launch_row_i(const KP& kp, const RowArgs& a, cudaStream_t st) {
   constexpr int N = 1 << L, RPC = rows_per_cta<T, L>();
-  const int rpc = a.rpc > 0 ? a.rpc : RPC;
-  const int grid = (N / 2 + 1 + rpc - 1) / rpc;
   if (a.rmode == RM_STAGE && !a.do_p1) {  // last stage: its own radix, the compiled launch shape
     constexpr int RPCX = rowx_rpc<T, L>();
     RowArgs ax = a;
     ax.rpc = 0;
-    return launch_pdl(k_row<T, L, rowx_radix<T, L>(), RPCX, rowx_depth<T, L>(), 0>,
+    return launch_pdl(k_row<T, L, rowx_radix<T, L>(), RPCX, rowx_depth<T, L>(), 0, RI>,
                       dim3((N / 2 + 1 + RPCX - 1) / RPCX), dim3(RPCX * rowx_group<T, L>()),
                       rowx_smem<T, L>(rowx_depth<T, L>()), st, kp, ax);
   }
-  return launch_pdl(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>, dim3(grid),
+  const int rpc = a.rpc > 0 ? a.rpc : RPC;
+  const int grid = (N / 2 + 1 + rpc - 1) / rpc;
+  return launch_pdl(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>(), RI>, dim3(grid),
                     dim3(rpc * row_group<T, L>()), row_smem<T, L>() / RPC * rpc, st, kp, a);
+}
+template <typename T, int L>
+cudaError_t launch_row_t(const KP& kp, const RowArgs& a, cudaStream_t st) {
+  switch (row_inst(a.rmode, a.fmode)) {
+    case RI_THETA_STAGE: return launch_row_i<T, L, RI_THETA_STAGE>(kp, a, st);
+    case RI_SCAL_STAGE: return launch_row_i<T, L, RI_SCAL_STAGE>(kp, a, st);
+    default: return launch_row_i<T, L, RI_ANY>(kp, a, st);
+  }
 }
 // Column passes of theta and of the scalars run instances compiled for their
 // mode alone (fewer registers live, fewer spills: N = 4096 FP32 theta column
 // pass 212 -> 204 us, scalar column pass 149 -> 134 us); the other modes run
-// the instance that chooses the mode at run time.
+// the instance that chooses the mode at run time (an instance for the
+// velocity pass alone was slower, 90 -> 92 us).
 template <typename T, int L, int CMX>
 cudaError_t launch_col_m(const KP& kp, const ColArgs& a, cudaStream_t st, int grid, int np) {
   constexpr int NP = pairs_per_cta<T, L>();
@@ -232,14 +248,23 @@ cudaError_t shape_max_t(int* rpc, int* np) {
   *np = pairs_per_cta<T, L>();
   return cudaSuccess;
 }
-template <typename T, int L>
-cudaError_t set_attrs_t() {
-  constexpr int RPC = rows_per_cta<T, L>(), NP = pairs_per_cta<T, L>();
-  cudaError_t e = cudaFuncSetAttribute(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>()>,
+template <typename T, int L, int RI>
+cudaError_t set_row_attrs_i() {
+  constexpr int RPC = rows_per_cta<T, L>();
+  cudaError_t e = cudaFuncSetAttribute(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>(), RI>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem<T, L>());
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_row<T, L, rowx_radix<T, L>(), rowx_rpc<T, L>(), rowx_depth<T, L>(), 0>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rowx_smem<T, L>(rowx_depth<T, L>()));
+  return cudaFuncSetAttribute(k_row<T, L, rowx_radix<T, L>(), rowx_rpc<T, L>(), rowx_depth<T, L>(), 0, RI>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rowx_smem<T, L>(rowx_depth<T, L>()));
+}
+template <typename T, int L>
+cudaError_t set_attrs_t() {
+  constexpr int NP = pairs_per_cta<T, L>();
+  cudaError_t e = set_row_attrs_i<T, L, RI_ANY>();
+  if (e != cudaSuccess) return e;
+  e = set_row_attrs_i<T, L, RI_THETA_STAGE>();
+  if (e != cudaSuccess) return e;
+  e = set_row_attrs_i<T, L, RI_SCAL_STAGE>();
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>(), CM_THETA>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem<T, L>());
