@@ -43,9 +43,19 @@ struct RowTab {
 
 enum FieldMode { FM_THETA = 0, FM_VEL = 1, FM_PHYS1 = 2, FM_SCAL = 3 };
 enum RowMode { RM_P1 = 0, RM_STAGE = 1, RM_RHS = 2, RM_SPEC = 3 };
-// Row-pass instances: one that reads its modes from the arguments, and the
-// stage passes of theta and of the scalars compiled for their modes alone.
-enum RowInst { RI_ANY = 0, RI_THETA_STAGE = 1, RI_SCAL_STAGE = 2 };
+// Row-pass instances: one that reads its modes from the arguments; the stage
+// passes of theta and of the scalars compiled for their modes alone (any
+// stage), or for their modes and one stage s = 1..4 (RI_THETA_S1 + s - 1,
+// RI_SCAL_S1 + s - 1).
+enum RowInst { RI_ANY = 0, RI_THETA_STAGE = 1, RI_SCAL_STAGE = 2, RI_THETA_S1 = 3, RI_SCAL_S1 = 7 };
+__host__ __device__ constexpr int ri_fmode(int ri) {
+  return (ri == RI_THETA_STAGE || (ri >= RI_THETA_S1 && ri < RI_SCAL_S1)) ? FM_THETA
+         : ((ri == RI_SCAL_STAGE || (ri >= RI_SCAL_S1 && ri < RI_SCAL_S1 + 4)) ? FM_SCAL : -1);
+}
+__host__ __device__ constexpr int ri_stage(int ri) {
+  return (ri >= RI_THETA_S1 && ri < RI_SCAL_S1) ? ri - RI_THETA_S1 + 1
+         : ((ri >= RI_SCAL_S1 && ri < RI_SCAL_S1 + 4) ? ri - RI_SCAL_S1 + 1 : 0);
+}
 enum AlphaKind { AK_GENERAL = 0, AK_ZERO = 1, AK_ONE = 2, AK_HALF = 3, AK_THREEHALF = 4, AK_TWO = 5, AK_MINUSONE = 6 };
 enum StageWrite { SW_NONE = 0, SW_FULL = 1, SW_RING = 2 };
 
@@ -307,7 +317,8 @@ template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX, int RI = RI
 __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int tile) {
   // modes fixed by the instance (RI), else read from the arguments
   const int rmode = RI == RI_ANY ? a.rmode : RM_STAGE;
-  const int fmode = RI == RI_THETA_STAGE ? FM_THETA : (RI == RI_SCAL_STAGE ? FM_SCAL : a.fmode);
+  const int fmode = ri_fmode(RI) >= 0 ? ri_fmode(RI) : a.fmode;
+  const int stage = ri_stage(RI) > 0 ? ri_stage(RI) : a.stage;
   using C = typename Cplx<T>::type;
   constexpr int N = 1 << LOG2N;
   constexpr int G = N / R;
@@ -352,8 +363,8 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
   } else {
     // stage pass: request this thread's theta_n / acc elements of the first
     // DEPTH chunks (own slots only, so no barrier is needed to consume them)
-    const bool pf_th = rmode == RM_STAGE && a.stage <= 3;
-    const bool pf_acc = rmode == RM_STAGE && a.stage >= 2;
+    const bool pf_th = rmode == RM_STAGE && stage <= 3;
+    const bool pf_acc = rmode == RM_STAGE && stage >= 2;
     const C* pth = reinterpret_cast<const C*>(a.th_n);
     const C* pacc = reinterpret_cast<const C*>(a.acc);
     auto issue = [&](int m) {
@@ -391,7 +402,7 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
       }
       return;
     }
-    const int s = a.stage;
+    const int s = stage;
     const bool scal = fmode == FM_SCAL;
     const C* st_in = reinterpret_cast<const C*>(s == 1 ? a.th_n : a.st_in);
     C* acc = reinterpret_cast<C*>(a.acc);

@@ -193,30 +193,52 @@ template <typename T> int multi_col_tiles(int log2n);
 // (pdl.cuh): the next pass's launch overlaps the tail of the current one.
 // The stage passes of theta and of the scalars run instances compiled for
 // their modes alone (RowInst: N = 4096 FP32 theta stage pass 290 -> 282 us,
-// scalar stage pass 193 -> 184 us); the other row passes run the instance
-// that reads its modes from the arguments.
+// scalar stage pass 193 -> 184 us) and, at N >= 2048, for their stage too
+// (theta 282 -> 268 us, scalars 184 -> 172 us);
+// the other row passes run the instance that reads its modes from the
+// arguments.
+template <typename T, int L>
+constexpr bool row_stage_insts() { return L >= 11; }
 constexpr int row_inst(int rmode, int fmode) {
   return rmode != RM_STAGE ? RI_ANY : (fmode == FM_THETA ? RI_THETA_STAGE : (fmode == FM_SCAL ? RI_SCAL_STAGE : RI_ANY));
 }
 template <typename T, int L, int RI>
 cudaError_t launch_row_i(const KP& kp, const RowArgs& a, cudaStream_t st) {
   constexpr int N = 1 << L, RPC = rows_per_cta<T, L>();
-  if (a.rmode == RM_STAGE && !a.do_p1) {  // last stage: its own radix, the compiled launch shape
-    constexpr int RPCX = rowx_rpc<T, L>();
-    RowArgs ax = a;
-    ax.rpc = 0;
-    return launch_pdl(k_row<T, L, rowx_radix<T, L>(), RPCX, rowx_depth<T, L>(), 0, RI>,
-                      dim3((N / 2 + 1 + RPCX - 1) / RPCX), dim3(RPCX * rowx_group<T, L>()),
-                      rowx_smem<T, L>(rowx_depth<T, L>()), st, kp, ax);
+  if constexpr (ri_stage(RI) == 0) {
+    if (a.rmode == RM_STAGE && !a.do_p1) {  // last stage: its own radix, the compiled launch shape
+      constexpr int RPCX = rowx_rpc<T, L>();
+      RowArgs ax = a;
+      ax.rpc = 0;
+      return launch_pdl(k_row<T, L, rowx_radix<T, L>(), RPCX, rowx_depth<T, L>(), 0, RI>,
+                        dim3((N / 2 + 1 + RPCX - 1) / RPCX), dim3(RPCX * rowx_group<T, L>()),
+                        rowx_smem<T, L>(rowx_depth<T, L>()), st, kp, ax);
+    }
   }
   const int rpc = a.rpc > 0 ? a.rpc : RPC;
   const int grid = (N / 2 + 1 + rpc - 1) / rpc;
   return launch_pdl(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>(), RI>, dim3(grid),
                     dim3(rpc * row_group<T, L>()), row_smem<T, L>() / RPC * rpc, st, kp, a);
 }
+template <typename T, int L, int RI0>
+cudaError_t launch_row_stage_i(const KP& kp, const RowArgs& a, cudaStream_t st) {
+  switch (a.stage) {
+    case 1: return launch_row_i<T, L, RI0>(kp, a, st);
+    case 2: return launch_row_i<T, L, RI0 + 1>(kp, a, st);
+    case 3: return launch_row_i<T, L, RI0 + 2>(kp, a, st);
+    default: return launch_row_i<T, L, RI0 + 3>(kp, a, st);
+  }
+}
 template <typename T, int L>
 cudaError_t launch_row_t(const KP& kp, const RowArgs& a, cudaStream_t st) {
-  switch (row_inst(a.rmode, a.fmode)) {
+  const int ri = row_inst(a.rmode, a.fmode);
+  if constexpr (row_stage_insts<T, L>()) {
+    if (a.do_p1 && a.stage >= 1 && a.stage <= 4) {
+      if (ri == RI_THETA_STAGE) return launch_row_stage_i<T, L, RI_THETA_S1>(kp, a, st);
+      if (ri == RI_SCAL_STAGE) return launch_row_stage_i<T, L, RI_SCAL_S1>(kp, a, st);
+    }
+  }
+  switch (ri) {
     case RI_THETA_STAGE: return launch_row_i<T, L, RI_THETA_STAGE>(kp, a, st);
     case RI_SCAL_STAGE: return launch_row_i<T, L, RI_SCAL_STAGE>(kp, a, st);
     default: return launch_row_i<T, L, RI_ANY>(kp, a, st);
@@ -253,9 +275,20 @@ cudaError_t set_row_attrs_i() {
   constexpr int RPC = rows_per_cta<T, L>();
   cudaError_t e = cudaFuncSetAttribute(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>(), RI>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem<T, L>());
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_row<T, L, rowx_radix<T, L>(), rowx_rpc<T, L>(), rowx_depth<T, L>(), 0, RI>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rowx_smem<T, L>(rowx_depth<T, L>()));
+  if constexpr (ri_stage(RI) == 0) {  // the last-stage kernel runs the mode instances only
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_row<T, L, rowx_radix<T, L>(), rowx_rpc<T, L>(), rowx_depth<T, L>(), 0, RI>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rowx_smem<T, L>(rowx_depth<T, L>()));
+  }
+  return e;
+}
+template <typename T, int L, int RI0>
+cudaError_t set_row_stage_attrs_i() {
+  cudaError_t e = set_row_attrs_i<T, L, RI0>();
+  if (e == cudaSuccess) e = set_row_attrs_i<T, L, RI0 + 1>();
+  if (e == cudaSuccess) e = set_row_attrs_i<T, L, RI0 + 2>();
+  if (e == cudaSuccess) e = set_row_attrs_i<T, L, RI0 + 3>();
+  return e;
 }
 template <typename T, int L>
 cudaError_t set_attrs_t() {
@@ -266,6 +299,12 @@ cudaError_t set_attrs_t() {
   if (e != cudaSuccess) return e;
   e = set_row_attrs_i<T, L, RI_SCAL_STAGE>();
   if (e != cudaSuccess) return e;
+  if constexpr (row_stage_insts<T, L>()) {
+    e = set_row_stage_attrs_i<T, L, RI_THETA_S1>();
+    if (e != cudaSuccess) return e;
+    e = set_row_stage_attrs_i<T, L, RI_SCAL_S1>();
+    if (e != cudaSuccess) return e;
+  }
   e = cudaFuncSetAttribute(k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>(), CM_THETA>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem<T, L>());
   if (e != cudaSuccess) return e;
