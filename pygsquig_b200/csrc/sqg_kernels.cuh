@@ -46,11 +46,20 @@ enum RowMode { RM_P1 = 0, RM_STAGE = 1, RM_RHS = 2, RM_SPEC = 3 };
 // Row-pass instances: one that reads its modes from the arguments; the stage
 // passes of theta and of the scalars compiled for their modes alone (any
 // stage), or for their modes and one stage s = 1..4 (RI_THETA_S1 + s - 1,
-// RI_SCAL_S1 + s - 1).
-enum RowInst { RI_ANY = 0, RI_THETA_STAGE = 1, RI_SCAL_STAGE = 2, RI_THETA_S1 = 3, RI_SCAL_S1 = 7 };
+// RI_SCAL_S1 + s - 1); the input passes (RM_P1) of theta, of the scalars and
+// of the velocity.
+enum RowInst {
+  RI_ANY = 0, RI_THETA_STAGE = 1, RI_SCAL_STAGE = 2, RI_THETA_S1 = 3, RI_SCAL_S1 = 7,
+  RI_THETA_P1 = 11, RI_SCAL_P1 = 12, RI_VEL_P1 = 13
+};
 __host__ __device__ constexpr int ri_fmode(int ri) {
-  return (ri == RI_THETA_STAGE || (ri >= RI_THETA_S1 && ri < RI_SCAL_S1)) ? FM_THETA
-         : ((ri == RI_SCAL_STAGE || (ri >= RI_SCAL_S1 && ri < RI_SCAL_S1 + 4)) ? FM_SCAL : -1);
+  return (ri == RI_THETA_STAGE || ri == RI_THETA_P1 || (ri >= RI_THETA_S1 && ri < RI_SCAL_S1)) ? FM_THETA
+         : ((ri == RI_SCAL_STAGE || ri == RI_SCAL_P1 || (ri >= RI_SCAL_S1 && ri < RI_SCAL_S1 + 4))
+                ? FM_SCAL
+                : (ri == RI_VEL_P1 ? FM_VEL : -1));
+}
+__host__ __device__ constexpr int ri_rmode(int ri) {
+  return ri == RI_ANY ? -1 : (ri >= RI_THETA_P1 ? RM_P1 : RM_STAGE);
 }
 __host__ __device__ constexpr int ri_stage(int ri) {
   return (ri >= RI_THETA_S1 && ri < RI_SCAL_S1) ? ri - RI_THETA_S1 + 1
@@ -316,7 +325,7 @@ __device__ __forceinline__ void row_fields(const KP& kp, const RowArgs& a, HA ha
 template <typename T, int LOG2N, int R, int RPC, int DEPTH, int NFX, int RI = RI_ANY>
 __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int tile) {
   // modes fixed by the instance (RI), else read from the arguments
-  const int rmode = RI == RI_ANY ? a.rmode : RM_STAGE;
+  const int rmode = ri_rmode(RI) >= 0 ? ri_rmode(RI) : a.rmode;
   const int fmode = ri_fmode(RI) >= 0 ? ri_fmode(RI) : a.fmode;
   const int stage = ri_stage(RI) > 0 ? ri_stage(RI) : a.stage;
   using C = typename Cplx<T>::type;

@@ -200,12 +200,14 @@ template <typename T> int multi_col_tiles(int log2n);
 template <typename T, int L>
 constexpr bool row_stage_insts() { return L >= 11; }
 constexpr int row_inst(int rmode, int fmode) {
+  if (rmode == RM_P1)
+    return fmode == FM_THETA ? RI_THETA_P1 : (fmode == FM_SCAL ? RI_SCAL_P1 : (fmode == FM_VEL ? RI_VEL_P1 : RI_ANY));
   return rmode != RM_STAGE ? RI_ANY : (fmode == FM_THETA ? RI_THETA_STAGE : (fmode == FM_SCAL ? RI_SCAL_STAGE : RI_ANY));
 }
 template <typename T, int L, int RI>
 cudaError_t launch_row_i(const KP& kp, const RowArgs& a, cudaStream_t st) {
   constexpr int N = 1 << L, RPC = rows_per_cta<T, L>();
-  if constexpr (ri_stage(RI) == 0) {
+  if constexpr (ri_stage(RI) == 0 && ri_rmode(RI) != RM_P1) {
     if (a.rmode == RM_STAGE && !a.do_p1) {  // last stage: its own radix, the compiled launch shape
       constexpr int RPCX = rowx_rpc<T, L>();
       RowArgs ax = a;
@@ -241,6 +243,9 @@ cudaError_t launch_row_t(const KP& kp, const RowArgs& a, cudaStream_t st) {
   switch (ri) {
     case RI_THETA_STAGE: return launch_row_i<T, L, RI_THETA_STAGE>(kp, a, st);
     case RI_SCAL_STAGE: return launch_row_i<T, L, RI_SCAL_STAGE>(kp, a, st);
+    case RI_THETA_P1: return launch_row_i<T, L, RI_THETA_P1>(kp, a, st);
+    case RI_SCAL_P1: return launch_row_i<T, L, RI_SCAL_P1>(kp, a, st);
+    case RI_VEL_P1: return launch_row_i<T, L, RI_VEL_P1>(kp, a, st);
     default: return launch_row_i<T, L, RI_ANY>(kp, a, st);
   }
 }
@@ -275,7 +280,7 @@ cudaError_t set_row_attrs_i() {
   constexpr int RPC = rows_per_cta<T, L>();
   cudaError_t e = cudaFuncSetAttribute(k_row<T, L, row_radix<T, L>(), RPC, row_depth<T, L>(), row_nfx<T, L>(), RI>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem<T, L>());
-  if constexpr (ri_stage(RI) == 0) {  // the last-stage kernel runs the mode instances only
+  if constexpr (ri_stage(RI) == 0 && ri_rmode(RI) != RM_P1) {  // the last-stage kernel: the stage instances
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_row<T, L, rowx_radix<T, L>(), rowx_rpc<T, L>(), rowx_depth<T, L>(), 0, RI>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rowx_smem<T, L>(rowx_depth<T, L>()));
@@ -298,6 +303,12 @@ cudaError_t set_attrs_t() {
   e = set_row_attrs_i<T, L, RI_THETA_STAGE>();
   if (e != cudaSuccess) return e;
   e = set_row_attrs_i<T, L, RI_SCAL_STAGE>();
+  if (e != cudaSuccess) return e;
+  e = set_row_attrs_i<T, L, RI_THETA_P1>();
+  if (e != cudaSuccess) return e;
+  e = set_row_attrs_i<T, L, RI_SCAL_P1>();
+  if (e != cudaSuccess) return e;
+  e = set_row_attrs_i<T, L, RI_VEL_P1>();
   if (e != cudaSuccess) return e;
   if constexpr (row_stage_insts<T, L>()) {
     e = set_row_stage_attrs_i<T, L, RI_THETA_S1>();
