@@ -863,6 +863,10 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
       col_fetch<T, LOG2N, R, NP, NBUF>(xb + fb1s * fstride, y0, 3, smem, np);
     }
     cp_async_commit();
+    if (NBUF == 3 && nround == 2) {  // round 2's first field lands in the third buffer during round 1
+      col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa1 * fstride, y0, 2, smem, np);
+      cp_async_commit();
+    }
   }
   if (cmode == CM_FWD) {
     const T* f = reinterpret_cast<const T*>(a.in_real);
@@ -905,15 +909,20 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
     for (int rd = 0; rd < nround; ++rd) {
       if (rd == 1) {
         __syncthreads();  // round-1 buffers free
-        col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa1 * fstride, y0, 0, smem, np);
-        col_fetch<T, LOG2N, R, NP, NBUF>(xh + fb1 * fstride, y0, 1, smem, np);
+        if (NBUF != 3) col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa1 * fstride, y0, 0, smem, np);
+        col_fetch<T, LOG2N, R, NP, NBUF>(xh + fb1 * fstride, y0, NBUF == 3 ? 0 : 1, smem, np);
         cp_async_commit();
       }
-      cp_async_wait<0>();
+      if (NBUF == 3 && rd == 0 && nround == 2) cp_async_wait<1>();  // the third buffer's copies may still fly
+      else cp_async_wait<0>();
       __syncthreads();
       C V[2][R];
-      col_first_load<T, LOG2N, R>(gbuf, j, V[0]);
-      col_first_load<T, LOG2N, R>(gbuf + SZ, j, V[1]);
+      // buffers of the round's two fields; the transforms exchange through
+      // buffers 0 and 1 (fft_multi synchronises before its first write)
+      const C* b0 = (NBUF == 3 && rd == 1) ? gbuf + 2 * SZ : gbuf;
+      const C* b1 = (NBUF == 3 && rd == 1) ? gbuf : gbuf + SZ;
+      col_first_load<T, LOG2N, R>(b0, j, V[0]);
+      col_first_load<T, LOG2N, R>(b1, j, V[1]);
       fft_multi<T, LOG2N, R, +1, 2>(V, gbuf, SZ, j, tw);
       if (cmode == CM_THETA) {
 #pragma unroll

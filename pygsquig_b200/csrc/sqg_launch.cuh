@@ -254,11 +254,17 @@ cudaError_t launch_row_t(const KP& kp, const RowArgs& a, cudaStream_t st) {
 // pass 212 -> 204 us, scalar column pass 149 -> 134 us); the other modes run
 // the instance that chooses the mode at run time (an instance for the
 // velocity pass alone was slower, 90 -> 92 us).
+// Field buffers per column pair of a mode instance: theta's radix-16 pass at
+// N = 4096 keeps a third, which receives round 2's first field during round 1.
+template <typename T, int L, int CMX>
+constexpr int col_nbuf_m() { return (CMX == CM_THETA && col_radix<T, L>() == 16 && L == 12) ? 3 : col_nbuf<T, L>(); }
+template <typename T, int L, int CMX>
+size_t col_smem_m() { return col_smem<T, L>() / col_nbuf<T, L>() * col_nbuf_m<T, L, CMX>(); }
 template <typename T, int L, int CMX>
 cudaError_t launch_col_m(const KP& kp, const ColArgs& a, cudaStream_t st, int grid, int np) {
   constexpr int NP = pairs_per_cta<T, L>();
-  return launch_pdl(k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>(), CMX>, dim3(grid),
-                    dim3(np * col_group<T, L>()), col_smem<T, L>() / NP * np, st, kp, a);
+  return launch_pdl(k_col<T, L, col_radix<T, L>(), NP, col_nbuf_m<T, L, CMX>(), CMX>, dim3(grid),
+                    dim3(np * col_group<T, L>()), col_smem_m<T, L, CMX>() / NP * np, st, kp, a);
 }
 template <typename T, int L>
 cudaError_t launch_col_t(const KP& kp, const ColArgs& a, cudaStream_t st, bool ring_only) {
@@ -316,8 +322,8 @@ cudaError_t set_attrs_t() {
     e = set_row_stage_attrs_i<T, L, RI_SCAL_S1>();
     if (e != cudaSuccess) return e;
   }
-  e = cudaFuncSetAttribute(k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>(), CM_THETA>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem<T, L>());
+  e = cudaFuncSetAttribute(k_col<T, L, col_radix<T, L>(), NP, col_nbuf_m<T, L, CM_THETA>(), CM_THETA>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem_m<T, L, CM_THETA>());
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_col<T, L, col_radix<T, L>(), NP, col_nbuf<T, L>(), CM_SCAL>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem<T, L>());
