@@ -421,6 +421,12 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
     const C* src_h = reinterpret_cast<const C*>(a.src_h);
     const double dt = kp.dt;
     const bool explicit_lin = (kp.scheme == 0);
+    // the scalar's source term is read one chunk ahead, ahead of the wait
+    // for the chunk's prefetched values, so that its latency overlaps the
+    // element updates of the chunk before
+    const bool use_src = scal && src_h != nullptr;
+    C sh_next = mkc<C>(0, 0);
+    if (use_src) sh_next = src_h[(size_t)p * N + j];
 #pragma unroll
     for (int m = 0; m < R; ++m) {
       const int iy = j + m * G;
@@ -428,6 +434,8 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
       const size_t e1 = (size_t)p * N + iy;
       const size_t e2 = (size_t)pp * N + iyp;
       const int my = mode_abs(iy, N);
+      const C sh = sh_next;
+      if (use_src && m + 1 < R) sh_next = src_h[(size_t)p * N + iy + G];
       cp_async_wait<DEPTH - 1>();  // chunk m has landed (groups are issued in order)
       const C* slot = pf + (size_t)(m % DEPTH) * 4 * G + j;
       const double kyd = wavenumber(kp, iy);
@@ -447,8 +455,7 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
       C J1 = v[m];
       C n1 = mkc<C>(-dmask * J1.x, -dmask * J1.y);
       C n2 = mkc<C>(-dmask * J1.x, dmask * J1.y);  // conj
-      if (scal && src_h) {
-        C sh = src_h[(size_t)p * N + iy];
+      if (use_src) {
         n1 = cadd(n1, sh);
         n2 = cadd(n2, cconj(sh));
       }
