@@ -278,8 +278,9 @@ int sqg_ensemble_multistep(sqg_ensemble* ensemble, int32_t n_steps, double dt, i
 int sqg_ensemble_last_launch_count(const sqg_ensemble* ensemble, int64_t* launches);
 int sqg_ensemble_destroy(sqg_ensemble* ensemble);
 
-/* Reads and clears the sticky status flags (bit 0: non-finite value seen).
- * Synchronises the stream. */
+/* Reads and clears the sticky status flags (bit 0: non-finite value seen;
+ * bit 1: a column pass's TMA tile copies did not complete within its bounded
+ * wait, so its results are not valid).  Synchronises the stream. */
 int sqg_check_status(sqg_plan* plan, uint32_t* flags, void* stream);
 
 /* Number of kernel launches the last sqg_step / sqg_multistep issued. */

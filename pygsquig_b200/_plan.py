@@ -294,9 +294,14 @@ class Plan:
         return self.shape()
 
     def check_status(self) -> int:
+        """Reads and clears the plan's status flags; returns bit 0 (non-finite
+        value seen).  Bit 1 (a column pass's tile copies did not complete
+        within the wait limit) raises."""
         f = C.c_uint32()
         _lib.check(self._lib.sqg_check_status(self._h, C.byref(f), _stream_ptr()))
-        return int(f.value)
+        if int(f.value) & 2:
+            raise RuntimeError("column pass: TMA tile copies did not complete within the wait limit")
+        return int(f.value) & 1
 
     TIMING_KINDS = ("row_inverse", "row_stage", "col_theta", "row_scalar", "col_scalar", "other", "row_last",
                     "row_vel", "col_vel", "row_scalar_inverse")

@@ -23,7 +23,7 @@ CSRC = os.path.join(HERE, "csrc")
 _INST = [f"sqg_inst_{t}_{r}.cu" for t in ("f32", "f64") for r in "abc"] + ["sqg_inst_multi.cu"]
 SRCS = [os.path.join(CSRC, f) for f in ["sqg_capi.cu"] + _INST + ["closure_conv.cu", "closure_ops.cu"]]
 # headers each unit includes (a change rebuilds the unit)
-_PASS_HDRS = ["pdl.cuh", "sqg_fft.cuh", "sqg_kernels.cuh", "sqg_launch.cuh"]
+_PASS_HDRS = ["pdl.cuh", "sqg_fft.cuh", "sqg_tma.cuh", "sqg_kernels.cuh", "sqg_launch.cuh"]
 DEPS = {
     "sqg_capi.cu": _PASS_HDRS + ["sqg_aux.cuh", "../../include/sqg.h"],
     "closure_conv.cu": ["pdl.cuh", "closure_act.cuh", "../../include/sqg_closure.h"],

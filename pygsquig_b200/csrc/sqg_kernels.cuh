@@ -26,6 +26,7 @@
 #pragma once
 #include "pdl.cuh"
 #include "sqg_fft.cuh"
+#include "sqg_tma.cuh"
 
 namespace sqg {
 
@@ -332,7 +333,7 @@ __device__ __forceinline__ void row_body(const KP& kp, const RowArgs& a, int til
   constexpr int N = 1 << LOG2N;
   constexpr int G = N / R;
   constexpr int H = N / 2;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* smem = reinterpret_cast<C*>(smem_raw);
   const int grp = threadIdx.x / G;
   const int j = threadIdx.x - grp * G;
@@ -686,6 +687,8 @@ struct ColArgs {
   int herm_ord[4];          // ordinals of (0,0),(N/2,0),(0,N/2),(N/2,N/2) or -1
   double* ring_scale_out;   // [4]
   int np;                   // column pairs per CTA (0: the compiled maximum NP)
+  int tma;                  // 1: the half columns of xh arrive as TMA tiles through the
+                            // kernel's tensor map (fields 0.. of the map = xh + f (N/2+1) N)
 };
 
 // Velocity u + i v of the scalar passes in physical space, stored
@@ -709,8 +712,15 @@ __device__ __forceinline__ void load_pair(const double2* p, double2& a, double2&
 // Slots of one field buffer of a column group: the raw half columns of the
 // pair, interleaved by row -- slot 2 kx = x(kx, ya), slot 2 kx + 1 =
 // x(kx, ya + 1) for kx = 0..N/2 -- later reused as the FFT exchange buffer.
-// SZ is even, so every buffer starts on a 16-byte boundary.
-template <int N, int R> struct ColBuf { static constexpr int SZ = (spad_size<R>(N) + 2 + 1) & ~1; };
+// SZ is even, so every buffer starts on a 16-byte boundary; from
+// N = kColTmaMinN on (the sizes whose column passes may take their half
+// columns as TMA tiles) a multiple of 16 elements, so that every buffer and
+// every 256-row box of it starts on a 128-byte boundary.
+constexpr int kColTmaMinN = 1024;
+template <int N, int R> struct ColBuf {
+  static constexpr int SZ0 = (spad_size<R>(N) + 2 + 1) & ~1;
+  static constexpr int SZ = N >= kColTmaMinN ? (SZ0 + 15) & ~15 : SZ0;
+};
 
 // 16-byte asynchronous global -> shared copy (both addresses 16-byte aligned).
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -724,16 +734,50 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 // float, two in double).  Copy unit u = (row kx, pair q, part): part fastest,
 // then the pair, so consecutive threads read a row's 16 np contiguous bytes
 // and write consecutive 16-byte slots (shifts only: np is a power of two).
+//
+// With a tensor map (tm, field fidx of its stack): rows 0..N/2-1 of each pair
+// arrive as np x N/(2 BH) TMA boxes of BH rows, issued by the lanes of warp 0
+// after lane 0 has added their bytes to the group's mbarrier phase (the
+// group's one arrival comes from col_commit); row N/2 is one cp.async per
+// pair and 16 bytes, as before.
 template <typename T, int LOG2N, int R, int NP, int NBUF>
 __device__ __forceinline__ void col_fetch(const typename Cplx<T>::type* __restrict__ f, int y0, int buf,
-                                          typename Cplx<T>::type* smem, int np) {
+                                          typename Cplx<T>::type* smem, int np, const CUtensorMap* tm = nullptr,
+                                          int fidx = 0, uint64_t* bar = nullptr) {
   using C = typename Cplx<T>::type;
   constexpr int N = 1 << LOG2N, H = N / 2, SZ = ColBuf<N, R>::SZ;
   constexpr int LC = sizeof(C) == 16 ? 1 : 0;  // log2(16-byte copies per row of a pair)
   const int ls = LC + (31 - __clz(np));        // log2(copy units per row)
-  const int units = (H + 1) << ls;
   unsigned char* zb = reinterpret_cast<unsigned char*>(smem + (size_t)buf * SZ);
   const unsigned char* gb = reinterpret_cast<const unsigned char*>(f + y0);
+  if constexpr (N >= kColTmaMinN) {
+    if (tm) {
+      constexpr int BH = H < 256 ? H : 256;  // rows per box
+      constexpr int NB = H / BH;             // boxes per pair
+      constexpr uint32_t kBoxBytes = BH * 2 * sizeof(C);
+      static_assert((SZ * sizeof(C)) % 128 == 0 && kBoxBytes % 128 == 0, "TMA boxes start on 128-byte boundaries");
+      if (threadIdx.x < 32) {
+        if (threadIdx.x == 0) tma_bar_expect(bar, (uint32_t)(np * NB) * kBoxBytes);
+        __syncwarp();
+        tma_proxy_fence();  // the block's earlier use of the buffers comes before the tile writes
+        for (int b = threadIdx.x; b < np * NB; b += 32) {
+          const int q = b / NB, c = b - q * NB;
+          tma_load_3d(zb + ((size_t)q * NBUF * SZ + 2 * BH * c) * sizeof(C), tm, bar,
+                      (y0 + 2 * q) * (int)(sizeof(C) / 4), BH * c, fidx);
+        }
+      }
+      // row H: one 16-byte unit (float) or two (double) per pair
+      const int units = 1 << ls;
+      for (int u = threadIdx.x; u < units; u += blockDim.x) {
+        const int part = u & ((1 << LC) - 1);
+        const int q = u >> LC;
+        cp_async16(zb + ((size_t)q * NBUF * SZ + 2 * H) * sizeof(C) + part * 16,
+                   gb + ((size_t)H * N + 2 * q) * sizeof(C) + part * 16);
+      }
+      return;
+    }
+  }
+  const int units = (H + 1) << ls;
   for (int u = threadIdx.x; u < units; u += blockDim.x) {
     const int part = u & ((1 << LC) - 1);
     const int q = (u >> LC) & (np - 1);
@@ -770,20 +814,44 @@ __device__ void ring_reduce(const KP& kp, const ColArgs& a);
 // two fields (large N in float64, where four buffers do not fit).
 // CMX >= 0: an instance compiled for that column mode alone (the other
 // modes' branches fold away); -1: every mode, chosen by a.cmode at run time.
+//
+// tm (non-null only from N = kColTmaMinN on, never in CM_SCALV): the field
+// stack xh as a tensor map; the half columns then arrive as TMA tiles (a
+// commit group's tiles complete on mbarrier colbar[g], one phase per group),
+// and a wait that runs out sets kStatusTmaTimeout in kp.status.
 template <typename T, int LOG2N, int R, int NP, int NBUF, int CMX = -1>
-__device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int tile, int ntiles) {
+__device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int tile, int ntiles,
+                                         const CUtensorMap* tm = nullptr) {
   using C = typename Cplx<T>::type;
   constexpr int N = 1 << LOG2N;
   constexpr int G = N / R;
   constexpr int H = N / 2;
   constexpr int SZ = ColBuf<N, R>::SZ;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* smem = reinterpret_cast<C*>(smem_raw);
   const int cmode = CMX >= 0 ? CMX : a.cmode;
   if ((CMX < 0 || CMX == CM_THETA) && a.ring_cta && tile == ntiles - 1) {
     ring_reduce<T, LOG2N>(kp, a);
     return;
   }
+  __shared__ uint64_t colbar[2];
+  if constexpr (N < kColTmaMinN) tm = nullptr;
+  if (cmode == CM_SCALV || (tma_smem_u32(smem_raw) & 127u) != 0u) tm = nullptr;
+  if (tm && threadIdx.x == 0) {
+    tma_bar_init(&colbar[0]);
+    tma_bar_init(&colbar[1]);
+    tma_bar_init_fence();
+  }
+  // a commit group of copies: the cp.async group and, with tiles, the one
+  // arrival of mbarrier g's phase
+  auto commit = [&](int g) {
+    cp_async_commit();
+    if (tm && threadIdx.x == 0) tma_bar_arrive(&colbar[g]);
+  };
+  // after the cp.async wait and a block barrier: the tiles of group g
+  auto tile_wait = [&](int g, uint32_t parity) {
+    if (tm && !tma_bar_wait(&colbar[g], parity) && kp.status) atomicOr(kp.status, kStatusTmaTimeout);
+  };
   const int grp = threadIdx.x / G;
   const int j = threadIdx.x - grp * G;
   const int np = a.np > 0 ? a.np : NP;       // launch shape (autotuned), <= NP
@@ -800,11 +868,12 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
     // u + i v for the scalar passes, column-pair-major (uv_index): both
     // fields transformed together, one 16-byte (float) or two 16-byte
     // (double) stores per thread and row
-    col_fetch<T, LOG2N, R, NP, NBUF>(xh, y0, 0, smem, np);
-    col_fetch<T, LOG2N, R, NP, NBUF>(xh + fstride, y0, 1, smem, np);
-    cp_async_commit();
+    col_fetch<T, LOG2N, R, NP, NBUF>(xh, y0, 0, smem, np, tm, 0, &colbar[0]);
+    col_fetch<T, LOG2N, R, NP, NBUF>(xh + fstride, y0, 1, smem, np, tm, 1, &colbar[0]);
+    commit(0);
     cp_async_wait<0>();
     __syncthreads();
+    tile_wait(0, 0);
     C V[2][R];
     col_first_load<T, LOG2N, R>(gbuf, j, V[0]);
     col_first_load<T, LOG2N, R>(gbuf + SZ, j, V[1]);
@@ -820,10 +889,11 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
   }
   if (cmode == CM_VEL || cmode == CM_PHYS1) {
     const int nf = cmode == CM_VEL ? 2 : 1;
-    for (int f = 0; f < nf; ++f) col_fetch<T, LOG2N, R, NP, NBUF>(xh + f * fstride, y0, f, smem, np);
-    cp_async_commit();
+    for (int f = 0; f < nf; ++f) col_fetch<T, LOG2N, R, NP, NBUF>(xh + f * fstride, y0, f, smem, np, tm, f, &colbar[0]);
+    commit(0);
     cp_async_wait<0>();
     __syncthreads();
+    tile_wait(0, 0);
     for (int f = 0; f < nf; ++f) {
       C* b = gbuf + f * SZ;
       col_first_load<T, LOG2N, R>(b, j, v);
@@ -863,16 +933,17 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
     // CM_SCALV: buffers (u, s_x, v, s_y) -- u, v from theta's xh, s_x, s_y from xh2
     const C* xb = cmode == CM_SCALV ? reinterpret_cast<const C*>(a.xh2) : xh;
     const int fb0s = cmode == CM_SCALV ? 0 : fb0, fb1s = cmode == CM_SCALV ? 1 : fb1;
-    col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa0 * fstride, y0, 0, smem, np);
-    col_fetch<T, LOG2N, R, NP, NBUF>(xb + fb0s * fstride, y0, 1, smem, np);
+    // (tm is null in CM_SCALV, so the tile fields are always fields of xh)
+    col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa0 * fstride, y0, 0, smem, np, tm, fa0, &colbar[0]);
+    col_fetch<T, LOG2N, R, NP, NBUF>(xb + fb0s * fstride, y0, 1, smem, np, tm, fb0s, &colbar[0]);
     if (NBUF == 4 && nround == 2) {
-      col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa1 * fstride, y0, 2, smem, np);
-      col_fetch<T, LOG2N, R, NP, NBUF>(xb + fb1s * fstride, y0, 3, smem, np);
+      col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa1 * fstride, y0, 2, smem, np, tm, fa1, &colbar[0]);
+      col_fetch<T, LOG2N, R, NP, NBUF>(xb + fb1s * fstride, y0, 3, smem, np, tm, fb1s, &colbar[0]);
     }
-    cp_async_commit();
+    commit(0);
     if (NBUF == 3 && nround == 2) {  // round 2's first field lands in the third buffer during round 1
-      col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa1 * fstride, y0, 2, smem, np);
-      cp_async_commit();
+      col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa1 * fstride, y0, 2, smem, np, tm, fa1, &colbar[1]);
+      commit(1);
     }
   }
   if (cmode == CM_FWD) {
@@ -886,6 +957,7 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
   if (NBUF == 4 && nround == 2) {
     cp_async_wait<0>();
     __syncthreads();
+    tile_wait(0, 0);
     C V[4][R];
 #pragma unroll
     for (int f = 0; f < 4; ++f) col_first_load<T, LOG2N, R>(gbuf + f * SZ, j, V[f]);
@@ -916,13 +988,15 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
     for (int rd = 0; rd < nround; ++rd) {
       if (rd == 1) {
         __syncthreads();  // round-1 buffers free
-        if (NBUF != 3) col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa1 * fstride, y0, 0, smem, np);
-        col_fetch<T, LOG2N, R, NP, NBUF>(xh + fb1 * fstride, y0, NBUF == 3 ? 0 : 1, smem, np);
-        cp_async_commit();
+        if (NBUF != 3) col_fetch<T, LOG2N, R, NP, NBUF>(xh + fa1 * fstride, y0, 0, smem, np, tm, fa1, &colbar[0]);
+        col_fetch<T, LOG2N, R, NP, NBUF>(xh + fb1 * fstride, y0, NBUF == 3 ? 0 : 1, smem, np, tm, fb1, &colbar[0]);
+        commit(0);  // the second phase of mbarrier 0
       }
       if (NBUF == 3 && rd == 0 && nround == 2) cp_async_wait<1>();  // the third buffer's copies may still fly
       else cp_async_wait<0>();
       __syncthreads();
+      tile_wait(0, (uint32_t)rd);
+      if (NBUF == 3 && rd == 1) tile_wait(1, 0);
       C V[2][R];
       // buffers of the round's two fields; the transforms exchange through
       // buffers 0 and 1 (fft_multi synchronises before its first write)
@@ -1078,9 +1152,9 @@ k_row(KP kp, RowArgs a) {
 
 template <typename T, int LOG2N, int R, int NP, int NBUF, int CMX = -1>
 __global__ void __launch_bounds__(NP * ((1 << LOG2N) / R), min_blocks_r<T, R>(NP * ((1 << LOG2N) / R)))
-k_col(KP kp, ColArgs a) {
+k_col(KP kp, ColArgs a, const __grid_constant__ CUtensorMap tm) {
   pdl_wait();
-  col_body<T, LOG2N, R, NP, NBUF, CMX>(kp, a, blockIdx.x, gridDim.x);
+  col_body<T, LOG2N, R, NP, NBUF, CMX>(kp, a, blockIdx.x, gridDim.x, a.tma ? &tm : nullptr);
 }
 
 // Batched forms: the member's parameters come from device arrays; members

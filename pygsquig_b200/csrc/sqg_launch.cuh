@@ -7,6 +7,8 @@
 // kernel instantiations build in parallel; sqg_capi.cu sees the declarations
 // and dispatches on log2(N) at run time.
 #pragma once
+#include <cstring>
+
 #include "sqg_kernels.cuh"
 
 namespace sqg {
@@ -145,7 +147,8 @@ size_t col_smem() {  // per column pair: NBUF buffers
 
 
 template <typename T, int L> cudaError_t launch_row_t(const KP& kp, const RowArgs& a, cudaStream_t st);
-template <typename T, int L> cudaError_t launch_col_t(const KP& kp, const ColArgs& a, cudaStream_t st, bool ring_only);
+template <typename T, int L>
+cudaError_t launch_col_t(const KP& kp, const ColArgs& a, cudaStream_t st, bool ring_only, const CUtensorMap* tm);
 template <typename T, int L> cudaError_t shape_max_t(int* rpc, int* np);
 template <typename T, int L> cudaError_t set_attrs_t();
 template <typename T, int L> cudaError_t launch_row_batch_t(const KP* kps, const RowArgs* as, int members, cudaStream_t st);
@@ -261,20 +264,30 @@ template <typename T, int L, int CMX>
 constexpr int col_nbuf_m() { return (CMX == CM_THETA && col_nbuf<T, L>() == 2 && L == 12) ? 3 : col_nbuf<T, L>(); }
 template <typename T, int L, int CMX>
 size_t col_smem_m() { return col_smem<T, L>() / col_nbuf<T, L>() * col_nbuf_m<T, L, CMX>(); }
+// tm (host copy): the tensor map of the field stack a.xh, passed as the
+// kernel's grid-constant parameter (null: the passes gather with cp.async).
 template <typename T, int L, int CMX>
-cudaError_t launch_col_m(const KP& kp, const ColArgs& a, cudaStream_t st, int grid, int np) {
+cudaError_t launch_col_m(const KP& kp, const ColArgs& a, cudaStream_t st, int grid, int np, const CUtensorMap* tm) {
   constexpr int NP = pairs_per_cta<T, L>();
+  CUtensorMap m;
+  std::memset(&m, 0, sizeof(m));
+  ColArgs b = a;
+  b.tma = 0;
+  if (tm && (1 << L) >= kColTmaMinN && a.cmode != CM_SCALV) {
+    m = *tm;
+    b.tma = 1;
+  }
   return launch_pdl(k_col<T, L, col_radix<T, L>(), NP, col_nbuf_m<T, L, CMX>(), CMX>, dim3(grid),
-                    dim3(np * col_group<T, L>()), col_smem_m<T, L, CMX>() / NP * np, st, kp, a);
+                    dim3(np * col_group<T, L>()), col_smem_m<T, L, CMX>() / NP * np, st, kp, b, m);
 }
 template <typename T, int L>
-cudaError_t launch_col_t(const KP& kp, const ColArgs& a, cudaStream_t st, bool ring_only) {
+cudaError_t launch_col_t(const KP& kp, const ColArgs& a, cudaStream_t st, bool ring_only, const CUtensorMap* tm) {
   constexpr int N = 1 << L, NP = pairs_per_cta<T, L>();
   const int np = a.np > 0 ? a.np : NP;
   const int grid = ring_only ? 1 : N / (2 * np) + (a.ring_cta ? 1 : 0);
-  if (a.cmode == CM_THETA) return launch_col_m<T, L, CM_THETA>(kp, a, st, grid, np);
-  if (a.cmode == CM_SCAL && !a.ring_cta) return launch_col_m<T, L, CM_SCAL>(kp, a, st, grid, np);
-  return launch_col_m<T, L, -1>(kp, a, st, grid, np);
+  if (a.cmode == CM_THETA) return launch_col_m<T, L, CM_THETA>(kp, a, st, grid, np, tm);
+  if (a.cmode == CM_SCAL && !a.ring_cta) return launch_col_m<T, L, CM_SCAL>(kp, a, st, grid, np, tm);
+  return launch_col_m<T, L, -1>(kp, a, st, grid, np, tm);
 }
 template <typename T, int L>
 cudaError_t shape_max_t(int* rpc, int* np) {
@@ -360,7 +373,7 @@ cudaError_t set_batch_attrs_t() {
 // Explicit instantiation of every launch function for one (T, log2 N).
 #define SQG_INSTANTIATE(T, L)                                                                               \
   template cudaError_t launch_row_t<T, L>(const KP&, const RowArgs&, cudaStream_t);                        \
-  template cudaError_t launch_col_t<T, L>(const KP&, const ColArgs&, cudaStream_t, bool);                  \
+  template cudaError_t launch_col_t<T, L>(const KP&, const ColArgs&, cudaStream_t, bool, const CUtensorMap*); \
   template cudaError_t shape_max_t<T, L>(int*, int*);                                                      \
   template cudaError_t set_attrs_t<T, L>();                                                                \
   template cudaError_t launch_row_batch_t<T, L>(const KP*, const RowArgs*, int, cudaStream_t);             \
