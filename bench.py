@@ -599,9 +599,13 @@ def main():
         N = 256 FP32 solve with the CNN closure on every RK stage (graph
         replay, forcing split into DNS-sized sub-steps) against the N = 2048
         FP32 DNS step (graph multistep), both with ring forcing kf = 20 and
-        CombinedDamping as in the closure experiment.  The spectral error
-        comes from the committed experiment report (its cost does not depend
-        on the weights)."""
+        CombinedDamping as in the closure experiment.  The spectral error is
+        measured in the run: free-running coarse solves with and without the
+        closure over 50 eddy times against the filtered DNS's time-mean E(k)
+        that the experiment recorded (the DNS spectrum itself is not re-run:
+        eight N = 2048 runs take far longer than a bench); the experiment
+        report's own figure (windows restarted from the filtered DNS) is
+        quoted beside it."""
         import math
 
         from pygsquig_b200.closure import experiment as X
@@ -648,9 +652,23 @@ def main():
                     "forcing_substeps": m, "weights": "trained" if os.path.exists(wpath) else "random (timing only)"})
         rpath = os.path.join(here, "closure_report.json")
         if os.path.exists(rpath):
-            r = json.load(open(rpath))["models"]["closure"]
-            out["max_rel_err_E_k_le_kf"] = r["max_rel_err_E_k_le_kf"]
-            out["error_source"] = "pygsquig_b200/closure/trained/closure_report.json"
+            rep = json.load(open(rpath))
+            out["report_max_rel_err_E_k_le_kf"] = rep["models"]["closure"]["max_rel_err_E_k_le_kf"]
+            out["report_source"] = ("pygsquig_b200/closure/trained/closure_report.json (coarse windows restarted "
+                                    "from the filtered DNS every 2 time units)")
+            # measured in this run: free-running coarse solves over 50 eddy times against the
+            # filtered DNS's time-mean E(k) that the experiment recorded
+            t_eddy = rep["eddy_time"]["value"]
+            live = {"closure": X.free_running_errors(cfg, clo, rep["E_dns"], eddy_time=t_eddy),
+                    "no_closure": X.free_running_errors(cfg, None, rep["E_dns"], eddy_time=t_eddy)}
+            out["max_rel_err_E_k_le_kf"] = live["closure"]["max_rel_err_E_k_le_kf"]
+            out["live_eval"] = {
+                "protocol": "free-running N = 256 solves (dt_c = 1e-3, forcing in DNS-sized sub-steps) from a "
+                            "seeded random-phase field with the DNS shell spectrum, 2 time units of spin-up, "
+                            "time mean of E(k) over 50 eddy times, per-shell relative error for k <= kf against "
+                            "the filtered N = 2048 DNS time mean",
+                **{k: {kk: v[kk] for kk in ("max_rel_err_E_k_le_kf", "worst_shell", "rel_err_E", "finite",
+                                            "t_avg", "steps")} for k, v in live.items()}}
         return out
 
     if args.workload == "ensemble96":
