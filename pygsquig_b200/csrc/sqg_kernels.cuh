@@ -849,8 +849,14 @@ __device__ __forceinline__ void col_body(const KP& kp, const ColArgs& a, int til
     if (tm && threadIdx.x == 0) tma_bar_arrive(&colbar[g]);
   };
   // after the cp.async wait and a block barrier: the tiles of group g
+  // (after a time-out the flag is set and the thread waits once more, also
+  // bounded, since the copies still in flight write this block's buffers;
+  // it then carries on, so that no thread leaves the block's barriers)
   auto tile_wait = [&](int g, uint32_t parity) {
-    if (tm && !tma_bar_wait(&colbar[g], parity) && kp.status) atomicOr(kp.status, kStatusTmaTimeout);
+    if (tm && !tma_bar_wait(&colbar[g], parity)) {
+      if (kp.status) atomicOr(kp.status, kStatusTmaTimeout);
+      tma_bar_wait(&colbar[g], parity);
+    }
   };
   const int grp = threadIdx.x / G;
   const int j = threadIdx.x - grp * G;
